@@ -1,0 +1,319 @@
+/*
+ * ufc_gpu.h -- C-ABI of the B200 implementation of UFC's implicit-static C3D8
+ * hot path: C3D8 element loop (linear elastic and J2), deterministic assembly
+ * into a device-built CSR stiffness, Jacobi-PCG (FP64, or FP32 inner
+ * iterations with FP64 residual refinement), Newton-Raphson increments, and the
+ * adjoint sensitivity.
+ *
+ * Every entry point returns an int32 status with the values of the reference's
+ * IF_STATUS_* codes (ufc_core/L1_IF/Error/IF_Err_Brg.f90:95-110); the message of
+ * the last failure is read with ufc_last_error (the reference's
+ * ErrorStatusType%message, ufc_core/L1_IF/Error/IF_Err_Def.f90:118-135).  No
+ * entry point exits, aborts or traps.
+ *
+ * The *_desc / *_arg structs are the batched, device-side counterparts of the
+ * reference's Desc/State/Algo/Ctx "*_Arg" bundles: fields marked [IN] are read,
+ * [OUT] are written.  Pointers are host or device memory as the struct's `mem`
+ * field (UFC_MEM_HOST / UFC_MEM_DEVICE) says; host buffers are borrowed for the
+ * duration of the call, device buffers are used in order on the context's
+ * stream.  A context owns all device memory it allocates (mesh, pattern, matrix
+ * values, solver work vectors, material state) and is not shared between
+ * threads; calls on one context are ordered on its stream.
+ *
+ * DOF numbering: eq = 3*node + component (ufc_core/L5_RT/Assembly/
+ * RT_Asm_DofMap.f90:172-249), nodes and elements 0-based unless index_base = 1.
+ * Element nodes in Abaqus order (ufc_core/L4_PH/Element/PH_Elem_ShapeFunc.f90:329-350).
+ * Voigt order (xx, yy, zz, gxy, gyz, gzx), engineering shear strains.
+ */
+#ifndef UFC_GPU_H
+#define UFC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* IF_STATUS_* (IF_Err_Brg.f90:95-110) */
+#define UFC_STATUS_OK 0
+#define UFC_STATUS_INVALID 1
+#define UFC_STATUS_ERROR 2
+#define UFC_STATUS_CONVERGED 3
+#define UFC_STATUS_NOT_CONVERGED 4
+#define UFC_STATUS_NOT_FOUND 5
+#define UFC_STATUS_WARN 6
+#define UFC_STATUS_MEM_ERROR 7
+#define UFC_STATUS_IO_ERROR 8
+#define UFC_STATUS_EXISTS 9
+#define UFC_STATUS_FATAL 10
+#define UFC_STATUS_UNSUPPORTED 11
+
+#define UFC_MEM_HOST 0
+#define UFC_MEM_DEVICE 1
+
+/* Material sub-model ids: PH_MAT_ELAS_SUB_ISO (ufc_core/L4_PH/Material/Elas/
+ * PH_Mat_Elas_Def.f90:24), PH_MAT_PLAST_SUB_J2_ISO (ufc_core/L4_PH/Material/
+ * Plast/PH_Mat_Plast_Def.f90:18). */
+#define UFC_MAT_ELASTIC_ISO 101
+#define UFC_MAT_J2_ISO 201
+
+/* NM_SOLV_METHOD_CG / NM_SOLV_PREC_* (ufc_core/L2_NM/Solver/NM_Solv_Def.f90:32-46) */
+#define UFC_SOLV_METHOD_CG 3
+#define UFC_SOLV_PREC_NONE 0
+#define UFC_SOLV_PREC_JACOBI 1
+
+/* Precision of the linear solve. */
+#define UFC_PRECISION_FP64 0        /* FP64 matrix, vectors and dot products      */
+#define UFC_PRECISION_FP32_REFINE 1 /* FP32 matrix and inner CG, FP64 solution and
+                                       FP64 residual replacement (refinement)      */
+#define UFC_PRECISION_FP32_MATRIX 2 /* FP32 matrix values only; FP64 CG vectors and
+                                       arithmetic, FP64 residual replacement       */
+
+/* Row-sum accumulator of the FP32_REFINE SpMV. */
+#define UFC_ACCUMULATE_STORAGE 0 /* FP32, like the stored values */
+#define UFC_ACCUMULATE_FP64 1    /* FP32 products summed in FP64 (same bytes moved) */
+
+/* Which matrix values ufc_elem_compute_ke builds (bit mask).  UFC_BUILD_FP32
+ * runs the element kernel in FP32; UFC_BUILD_FP32_ROUNDED instead rounds the
+ * FP64-assembled values to FP32 (implies UFC_BUILD_FP64); UFC_BUILD_FP32_DIFF
+ * stores the FP32 matrix in difference form: off-diagonal blocks rounded from
+ * FP64 and, in the diagonal slot, the FP64 block row sum S_i = sum_j K_ij, so
+ * that the SpMV evaluates y_i = sum_{j != i} K_ij (x_j - x_i) + S_i x_i, whose
+ * rounding error vanishes on rigid translations (implies UFC_BUILD_FP64). */
+#define UFC_BUILD_FP64 1
+#define UFC_BUILD_FP32 2
+#define UFC_BUILD_FP32_ROUNDED 4
+#define UFC_BUILD_FP32_DIFF 8
+
+/* FP32_REFINE policy at each FP64 residual replacement. */
+#define UFC_REFINE_KEEP_DIRECTION 0 /* keep the search direction (reliable update) */
+#define UFC_REFINE_RESTART 1        /* restart CG from the new residual (defect correction) */
+
+typedef struct ufc_ctx ufc_ctx;
+
+/* Mesh description: the L3 mesh plus PH_Elem_Desc of a C3D8 domain
+ * (ufc_core/L4_PH/Element/PH_Elem_Def.f90:329-355). */
+typedef struct {
+  int32_t n_nodes;       /* [IN] */
+  int32_t n_elems;       /* [IN] */
+  const double* coords;  /* [IN] [n_nodes][3] */
+  const int32_t* conn;   /* [IN] [n_elems][8], Abaqus node order */
+  int32_t index_base;    /* [IN] 0, or 1 for Fortran connectivity */
+  int32_t mem;           /* [IN] UFC_MEM_HOST / UFC_MEM_DEVICE */
+} ufc_mesh_desc;
+
+/* Material description: PH_Mat_Elas_Desc / PH_J2_Props with the props layout
+ * [E, nu] (101) or [E, nu, sigma_y0, H_iso] (201) of config/UMAT_Props_Layout.json. */
+typedef struct {
+  int32_t mat_model_id;  /* [IN] UFC_MAT_ELASTIC_ISO or UFC_MAT_J2_ISO */
+  int32_t nprops;        /* [IN] >= 2 (elastic) or >= 4 (J2) */
+  int32_t per_element;   /* [IN] 1: props[n_elems][nprops]; 0: props[nprops] for all */
+  const double* props;   /* [IN] */
+  int32_t mem;           /* [IN] */
+} ufc_material_desc;
+
+/* Dirichlet set: eliminated symmetrically (zero row and column, unit diagonal,
+ * lifted right-hand side) in place of the penalty of
+ * RT_Asm_ApplyBC_Displacement_Penalty (ufc_core/L5_RT/Assembly/RT_Asm_Solv.f90:427-483). */
+typedef struct {
+  int32_t n_fixed;       /* [IN] */
+  const int32_t* dofs;   /* [IN] [n_fixed] DOF ids (index_base of the mesh) */
+  const double* values;  /* [IN] [n_fixed] prescribed values, or NULL for zero */
+  int32_t mem;           /* [IN] */
+} ufc_bc_desc;
+
+/* Pattern summary returned by ufc_pattern_build. */
+typedef struct {
+  int64_t n_dof;          /* [OUT] 3 * n_nodes */
+  int64_t nnz;            /* [OUT] scalar CSR non-zeros = 9 * nnzb */
+  int64_t nnzb;           /* [OUT] 3x3 blocks */
+  int64_t sell_blocks;    /* [OUT] stored blocks incl. slice padding */
+  int32_t n_colors;       /* [OUT] element colours */
+  int32_t max_row_blocks; /* [OUT] */
+} ufc_pattern_info;
+
+/* Canonical CSR export: RT_CSRMatrix{rowPtr, colInd, values} of
+ * ufc_core/L2_NM/Matrix/NM_Assem_Sparse.f90:45-54. */
+typedef struct {
+  int32_t index_base;   /* [IN] 1 gives rowPtr(1) = 1 as the reference stores it */
+  int32_t mem;          /* [IN] */
+  int64_t* row_ptr;     /* [OUT] [n_dof+1] or NULL */
+  int32_t* col_ind;     /* [OUT] [nnz] or NULL */
+  double* values;       /* [OUT] [nnz] FP64 values or NULL */
+  float* values32;      /* [OUT] [nnz] FP32 values or NULL */
+} ufc_csr_export_arg;
+
+/* Batched PH_Element_Compute_Ke_Arg (PH_Elem_Def.f90:331-341) over every
+ * element, followed by the scatter of RT_Asm_GlobalStiffness
+ * (RT_Asm_Solv.f90:1762-1985).  For UFC_MAT_J2_ISO the per-Gauss-point
+ * consistent tangents of the last ufc_elem_compute_fint(update_state=1) are used. */
+typedef struct {
+  int32_t build;        /* [IN] UFC_BUILD_FP64 | UFC_BUILD_FP32 */
+  int32_t status;       /* [OUT] */
+  double elapsed_ms;    /* [OUT] device time of the assembly kernels */
+} ufc_elem_ke_arg;
+
+/* Batched PH_Element_Compute_Fe_Arg (PH_Elem_Def.f90:343-355) and
+ * RT_Asm_ComputeResidual (RT_Asm_Solv.f90:1311-1426) with the internal force
+ * F_int = sum_e int B^T sigma dV (PH_Elem_C3D8_IntForce, PH_Elem_C3D8.f90:734-757). */
+typedef struct {
+  const double* u;      /* [IN] [n_dof] displacement, prescribed values included */
+  const double* f_ext;  /* [IN] [n_dof] or NULL (zero) */
+  double* fint;         /* [OUT] [n_dof] F_int over every DOF, or NULL */
+  double* r;            /* [OUT] [n_dof] f_ext - F_int on free DOFs, 0 on fixed, or NULL */
+  int32_t mem;          /* [IN] */
+  int32_t update_state; /* [IN] J2: return-map every Gauss point from the committed
+                           state at u and keep the trial state and tangents */
+  double rnorm;         /* [OUT] ||r||_2 over the free DOFs (FP64) */
+  double fint_norm;     /* [OUT] ||F_int||_2 over every DOF */
+  int32_t status;       /* [OUT] */
+} ufc_elem_fe_arg;
+
+/* Batched PH_Mat_Update_Arg (ufc_core/L4_PH/Material/PH_Mat_KernelDefn.f90:18-59)
+ * / PH_J2_ComputeStress_Arg (PH_Mat_Plast_J2_Iso_Core.f90:119-126), one
+ * material point per entry, array-of-structs rows. */
+typedef struct {
+  int32_t mat_model_id;   /* [IN] */
+  int32_t n_points;       /* [IN] */
+  int32_t nprops;         /* [IN] */
+  int32_t props_per_point;/* [IN] 1: props[n_points][nprops]; 0: props[nprops] */
+  const double* props;    /* [IN] */
+  const double* stress_n; /* [IN] [n][6] committed stress */
+  const double* dstrain;  /* [IN] [n][6] strain increment */
+  const double* sdv_n;    /* [IN] [n][7] (eps_p_eq, eps_p[6]) or NULL (zero) */
+  double* stress;         /* [OUT] [n][6] */
+  double* sdv;            /* [OUT] [n][7] or NULL */
+  double* ddsdde;         /* [OUT] [n][36] row-major consistent tangent, or NULL */
+  int32_t* yielded;       /* [OUT] [n] or NULL */
+  int32_t mem;            /* [IN] */
+  int32_t status;         /* [OUT] */
+} ufc_mat_update_arg;
+
+/* NM_Solver_Algo (ufc_core/L2_NM/Solver/NM_Solv_Def.f90:86-100). */
+typedef struct {
+  int32_t method;         /* [IN] UFC_SOLV_METHOD_CG */
+  int32_t precond_type;   /* [IN] UFC_SOLV_PREC_JACOBI or UFC_SOLV_PREC_NONE */
+  int32_t max_iter;       /* [IN] */
+  int32_t precision_mode; /* [IN] UFC_PRECISION_FP64 or UFC_PRECISION_FP32_REFINE */
+  double tolerance;       /* [IN] stop when ||b - K x||_2 <= max(tolerance*||b||_2, abs_tolerance) */
+  double abs_tolerance;   /* [IN] */
+  double refine_delta;    /* [IN] FP32_REFINE: replace the FP32 residual by the FP64
+                             one whenever it fell by this factor (0: default 0.1) */
+  int32_t check_every;    /* [IN] iterations per launch batch between host checks (0: default) */
+  int32_t use_x0;         /* [IN] 1: x holds the initial guess; 0: x0 = 0 */
+  int32_t refine_policy;  /* [IN] UFC_REFINE_KEEP_DIRECTION or UFC_REFINE_RESTART */
+  int32_t accumulate;     /* [IN] FP32_REFINE: UFC_ACCUMULATE_STORAGE or UFC_ACCUMULATE_FP64 */
+} ufc_solver_algo;
+
+/* NM_Solver_State (ufc_core/L2_NM/Solver/NM_Solv_Def.f90:105-117). */
+typedef struct {
+  int32_t niter;           /* [OUT] CG iterations */
+  int32_t n_refine;        /* [OUT] FP64 residual replacements */
+  int32_t converged;       /* [OUT] */
+  int32_t convergence_flag;/* [OUT] 0 converged, 2 max-iter, 3 breakdown */
+  double rnorm;            /* [OUT] final ||b - K x||_2 / ||b||_2 in FP64 */
+  double initial_residual; /* [OUT] ||b - K x0||_2 */
+  double solve_time;       /* [OUT] ms, CUDA events around the device work */
+  int32_t fp64_iters;      /* [OUT] FP32 modes: FP64 iterations run after the FP32 run
+                              stalled or diverged (continued from its best iterate when
+                              FP64 values are assembled); included in niter */
+  int32_t reserved;
+} ufc_solver_state;
+
+/* One Newton-Raphson increment: RT_NLSolver_NewtonRaph
+ * (ufc_core/L5_RT/Solver/RT_Solv_Nonlin.f90:807-1002). */
+typedef struct {
+  const double* u_prescribed; /* [IN] [n_fixed] values of the Dirichlet DOFs at the end of the increment */
+  const double* f_ext;        /* [IN] [n_dof] or NULL */
+  int32_t mem;                /* [IN] */
+  int32_t max_iterations;     /* [IN] */
+  double tolerance_force;     /* [IN] ||R_free|| <= tol * max(||F_ext||, ||F_int||) */
+  ufc_solver_algo lin;        /* [IN] linear solver for K du = R */
+  int32_t iterations;         /* [OUT] */
+  int32_t converged;          /* [OUT] */
+  int32_t lin_iters_total;    /* [OUT] */
+  double residual_norm;       /* [OUT] final relative residual */
+  double res_hist[32];        /* [OUT] relative residual before each iteration's solve */
+  int32_t status;             /* [OUT] */
+} ufc_nr_arg;
+
+/* Device-time counters of the last ufc_pcg_solve (filled when instrumentation
+ * is on, see ufc_ctx_set_instrument). */
+typedef struct {
+  int32_t spmv_launches;
+  double spmv_ms;        /* sum of CUDA-event durations of the SpMV launches */
+  int64_t spmv_bytes;    /* algorithmic bytes of one SpMV launch */
+  int32_t precision;     /* UFC_PRECISION_* of the timed SpMV */
+  int64_t kernel_launches; /* kernels the last solve enqueued (always counted) */
+} ufc_timing_info;
+
+/* ---- context (replaces the reference's L0 global container g_ufc_global,
+ *      ufc_core/L0_Global/UFC_GlobalContainer_Core.f90) ---- */
+int ufc_ctx_create(int32_t device, ufc_ctx** ctx);
+int ufc_ctx_destroy(ufc_ctx* ctx);
+/* Use a caller-owned cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream); NULL = own stream. */
+int ufc_ctx_set_stream(ufc_ctx* ctx, void* cuda_stream);
+int ufc_ctx_set_instrument(ufc_ctx* ctx, int32_t on);
+/* ErrorStatusType%message (IF_Err_Def.f90:118-135) of the last failure. */
+int ufc_last_error(const ufc_ctx* ctx, char* buf, int32_t buflen);
+
+/* ---- model set-up ---- */
+int ufc_mesh_set(ufc_ctx* ctx, const ufc_mesh_desc* mesh);
+int ufc_material_set(ufc_ctx* ctx, const ufc_material_desc* mat);
+int ufc_bc_set(ufc_ctx* ctx, const ufc_bc_desc* bc);
+
+/* Device-built sorted-unique CSR pattern, once per mesh: replaces
+ * RT_CSR_FromTripletMerged (ufc_core/L5_RT/Solver/RT_Solv_Sparse.f90:336-445)
+ * and NM_COO_to_CSR (ufc_core/L2_NM/Matrix/NM_Mtx_Sparse.f90:164-222), plus the
+ * element colouring of RT_AsmColor_Build (ufc_core/L5_RT/Assembly/RT_Asm_Color.f90:36-182). */
+int ufc_pattern_build(ufc_ctx* ctx, ufc_pattern_info* info);
+int ufc_csr_export(ufc_ctx* ctx, const ufc_csr_export_arg* arg);
+
+/* ---- element / material ---- */
+int ufc_elem_compute_ke(ufc_ctx* ctx, ufc_elem_ke_arg* arg);
+int ufc_elem_compute_fint(ufc_ctx* ctx, ufc_elem_fe_arg* arg);
+int ufc_mat_update_batch(ufc_ctx* ctx, ufc_mat_update_arg* arg);
+/* Gauss-point stress ([n_elems][8][6]) and von Mises ([n_elems][8]) at u
+ * (PH_Elem_C3D8_EvalVonMises, PH_Elem_C3D8.f90:2768-2780); J2 models report the
+ * committed state and ignore u.  Either output may be NULL. */
+int ufc_stress_eval(ufc_ctx* ctx, const double* u, double* stress_gp, double* vm_gp, int32_t mem);
+
+/* ---- linear algebra ---- */
+/* y = K x with the assembled matrix of the given precision (RT_CSRMatrix_matvec,
+ * ufc_core/L2_NM/Matrix/NM_Assem_Sparse.f90:199-212).  UFC_PRECISION_FP32_REFINE
+ * takes float x/y; FP64 and FP32_MATRIX take double x/y. */
+int ufc_spmv(ufc_ctx* ctx, int32_t precision, const void* x, void* y, int32_t mem);
+/* Jacobi-PCG on the eliminated system K x = b: NM_Solver_PCG
+ * (ufc_core/L2_NM/Solver/NM_Solv_Core.f90:363-423) and iter_pcg
+ * (ufc_core/L2_NM/Solver/LinSolv/NM_Solv_IterSolver.f90:713-846).  b holds the
+ * lifted right-hand side (prescribed values on fixed DOFs).  Returns
+ * UFC_STATUS_NOT_CONVERGED when max_iter is reached. */
+int ufc_pcg_solve(ufc_ctx* ctx, const double* b, double* x, int32_t mem, const ufc_solver_algo* algo,
+                  ufc_solver_state* state);
+/* nrhs independent Jacobi-PCG solves sharing every SpMV (one matrix read per
+ * iteration for all right-hand sides).  B and X are [nrhs][n_dof]; states[nrhs]. */
+int ufc_pcg_solve_block(ufc_ctx* ctx, int32_t nrhs, const double* B, double* X, int32_t mem,
+                        const ufc_solver_algo* algo, ufc_solver_state* states);
+int ufc_last_timing(const ufc_ctx* ctx, ufc_timing_info* info);
+
+/* ---- nonlinear driver and material state (RT_Step_Exec.f90:415-600) ---- */
+int ufc_nr_increment(ufc_ctx* ctx, ufc_nr_arg* arg);
+int ufc_state_commit(ufc_ctx* ctx);
+int ufc_state_rollback(ufc_ctx* ctx);
+/* Current displacement held by the context ([n_dof]). */
+int ufc_get_displacement(ufc_ctx* ctx, double* u, int32_t mem);
+int ufc_set_displacement(ufc_ctx* ctx, const double* u, int32_t mem);
+/* Committed J2 state: eps_p_eq [n_elems*8], stress [n_elems*8][6], eps_p [n_elems*8][6]; any may be NULL. */
+int ufc_get_state(ufc_ctx* ctx, double* eps_p_eq, double* stress, double* eps_p, int32_t mem);
+
+/* ---- adjoint: dJ/dE_e = -sum_k lambda_k,e^T (dK_e/dE_e) u_k,e for nrhs pairs
+ * ([nrhs][n_dof]); replaces the stubs NM_AI_Adjoint_Solve
+ * (ufc_core/L2_NM/Solver/AI/NM_AI_AdjointAlgo.f90:116-136) and
+ * PH_Elem_dRdTheta_FD (ufc_core/L4_PH/Element/PH_Elem_dRdTheta.f90:59-78). ---- */
+int ufc_adjoint_sensitivity(ufc_ctx* ctx, int32_t nrhs, const double* U, const double* Lam, double* dJdE,
+                            int32_t mem);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UFC_GPU_H */

@@ -1,0 +1,204 @@
+!===============================================================================
+! ufc_gpu_brg.f90 -- ISO_C_BINDING interface to libufc_gpu.so (include/ufc_gpu.h)
+!
+! The Fortran side of the drop-in boundary: derived types with BIND(C) that
+! mirror the C structs field by field, and interfaces to the extern "C" entry
+! points, in the style of the reference's existing BIND(C) bridges
+! (ufc_core/L2_NM/Solver/LinSolv/NM_Solv_Dir.f90:19-47).  Status values are the
+! IF_STATUS_* codes of ufc_core/L1_IF/Error/IF_Err_Brg.f90:95-110.
+!
+! Not compiled in this repository (no Fortran compiler is available where it is
+! built); the C layouts it must match are checked by tests/test_abi.py.
+!===============================================================================
+MODULE ufc_gpu_brg
+  USE, INTRINSIC :: ISO_C_BINDING
+  IMPLICIT NONE
+  PRIVATE
+
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_MEM_HOST = 0, UFC_MEM_DEVICE = 1
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_MAT_ELASTIC_ISO = 101, UFC_MAT_J2_ISO = 201
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_SOLV_METHOD_CG = 3, UFC_SOLV_PREC_JACOBI = 1
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_PRECISION_FP64 = 0, UFC_PRECISION_FP32_REFINE = 1
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_BUILD_FP64 = 1, UFC_BUILD_FP32 = 2
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_BUILD_FP32_ROUNDED = 4, UFC_BUILD_FP32_DIFF = 8
+
+  TYPE, BIND(C), PUBLIC :: ufc_mesh_desc
+    INTEGER(C_INT32_T) :: n_nodes, n_elems
+    TYPE(C_PTR)        :: coords, conn          ! REAL(C_DOUBLE)(3,n_nodes), INTEGER(C_INT32_T)(8,n_elems)
+    INTEGER(C_INT32_T) :: index_base, mem       ! index_base = 1 for Fortran connectivity
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_material_desc
+    INTEGER(C_INT32_T) :: mat_model_id, nprops, per_element
+    TYPE(C_PTR)        :: props                 ! REAL(C_DOUBLE)(nprops[,n_elems])
+    INTEGER(C_INT32_T) :: mem
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_bc_desc
+    INTEGER(C_INT32_T) :: n_fixed
+    TYPE(C_PTR)        :: dofs, values
+    INTEGER(C_INT32_T) :: mem
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_pattern_info
+    INTEGER(C_INT64_T) :: n_dof, nnz, nnzb, sell_blocks
+    INTEGER(C_INT32_T) :: n_colors, max_row_blocks
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_csr_export_arg
+    INTEGER(C_INT32_T) :: index_base, mem
+    TYPE(C_PTR)        :: row_ptr, col_ind, values, values32
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_elem_ke_arg
+    INTEGER(C_INT32_T) :: build, status
+    REAL(C_DOUBLE)     :: elapsed_ms
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_elem_fe_arg
+    TYPE(C_PTR)        :: u, f_ext, fint, r
+    INTEGER(C_INT32_T) :: mem, update_state
+    REAL(C_DOUBLE)     :: rnorm, fint_norm
+    INTEGER(C_INT32_T) :: status
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_mat_update_arg
+    INTEGER(C_INT32_T) :: mat_model_id, n_points, nprops, props_per_point
+    TYPE(C_PTR)        :: props, stress_n, dstrain, sdv_n, stress, sdv, ddsdde, yielded
+    INTEGER(C_INT32_T) :: mem, status
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_solver_algo          ! NM_Solver_Algo
+    INTEGER(C_INT32_T) :: method = UFC_SOLV_METHOD_CG, precond_type = UFC_SOLV_PREC_JACOBI
+    INTEGER(C_INT32_T) :: max_iter = 100000, precision_mode = UFC_PRECISION_FP64
+    REAL(C_DOUBLE)     :: tolerance = 1.0D-10, abs_tolerance = 0.0D0, refine_delta = 0.0D0
+    INTEGER(C_INT32_T) :: check_every = 0, use_x0 = 0, refine_policy = 0, accumulate = 0
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_solver_state         ! NM_Solver_State
+    INTEGER(C_INT32_T) :: niter, n_refine, converged, convergence_flag
+    REAL(C_DOUBLE)     :: rnorm, initial_residual, solve_time
+    INTEGER(C_INT32_T) :: fp64_iters, reserved
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_nr_arg               ! RT_NLSolver_NewtonRaph, one increment
+    TYPE(C_PTR)           :: u_prescribed, f_ext
+    INTEGER(C_INT32_T)    :: mem, max_iterations
+    REAL(C_DOUBLE)        :: tolerance_force
+    TYPE(ufc_solver_algo) :: lin
+    INTEGER(C_INT32_T)    :: iterations, converged, lin_iters_total
+    REAL(C_DOUBLE)        :: residual_norm, res_hist(32)
+    INTEGER(C_INT32_T)    :: status
+  END TYPE
+
+  PUBLIC :: ufc_ctx_create, ufc_ctx_destroy, ufc_last_error, ufc_mesh_set, ufc_material_set, ufc_bc_set
+  PUBLIC :: ufc_pattern_build, ufc_csr_export, ufc_elem_compute_ke, ufc_elem_compute_fint
+  PUBLIC :: ufc_mat_update_batch, ufc_pcg_solve, ufc_pcg_solve_block, ufc_nr_increment
+  PUBLIC :: ufc_state_commit, ufc_state_rollback, ufc_get_displacement, ufc_adjoint_sensitivity
+
+  INTERFACE
+    INTEGER(C_INT) FUNCTION ufc_ctx_create(device, ctx) BIND(C, NAME='ufc_ctx_create')
+      IMPORT :: C_INT, C_INT32_T, C_PTR
+      INTEGER(C_INT32_T), VALUE :: device
+      TYPE(C_PTR), INTENT(OUT)  :: ctx
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_ctx_destroy(ctx) BIND(C, NAME='ufc_ctx_destroy')
+      IMPORT :: C_INT, C_PTR
+      TYPE(C_PTR), VALUE :: ctx
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_last_error(ctx, buf, buflen) BIND(C, NAME='ufc_last_error')
+      IMPORT :: C_INT, C_PTR, C_CHAR, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx
+      CHARACTER(KIND=C_CHAR)        :: buf(*)
+      INTEGER(C_INT32_T), VALUE     :: buflen
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_mesh_set(ctx, mesh) BIND(C, NAME='ufc_mesh_set')
+      IMPORT :: C_INT, C_PTR, ufc_mesh_desc
+      TYPE(C_PTR), VALUE               :: ctx
+      TYPE(ufc_mesh_desc), INTENT(IN)  :: mesh
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_material_set(ctx, mat) BIND(C, NAME='ufc_material_set')
+      IMPORT :: C_INT, C_PTR, ufc_material_desc
+      TYPE(C_PTR), VALUE                  :: ctx
+      TYPE(ufc_material_desc), INTENT(IN) :: mat
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_bc_set(ctx, bc) BIND(C, NAME='ufc_bc_set')
+      IMPORT :: C_INT, C_PTR, ufc_bc_desc
+      TYPE(C_PTR), VALUE            :: ctx
+      TYPE(ufc_bc_desc), INTENT(IN) :: bc
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_pattern_build(ctx, info) BIND(C, NAME='ufc_pattern_build')
+      IMPORT :: C_INT, C_PTR, ufc_pattern_info
+      TYPE(C_PTR), VALUE                   :: ctx
+      TYPE(ufc_pattern_info), INTENT(OUT)  :: info
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_csr_export(ctx, arg) BIND(C, NAME='ufc_csr_export')
+      IMPORT :: C_INT, C_PTR, ufc_csr_export_arg
+      TYPE(C_PTR), VALUE                   :: ctx
+      TYPE(ufc_csr_export_arg), INTENT(IN) :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_elem_compute_ke(ctx, arg) BIND(C, NAME='ufc_elem_compute_ke')
+      IMPORT :: C_INT, C_PTR, ufc_elem_ke_arg
+      TYPE(C_PTR), VALUE                  :: ctx
+      TYPE(ufc_elem_ke_arg), INTENT(INOUT) :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_elem_compute_fint(ctx, arg) BIND(C, NAME='ufc_elem_compute_fint')
+      IMPORT :: C_INT, C_PTR, ufc_elem_fe_arg
+      TYPE(C_PTR), VALUE                  :: ctx
+      TYPE(ufc_elem_fe_arg), INTENT(INOUT) :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_mat_update_batch(ctx, arg) BIND(C, NAME='ufc_mat_update_batch')
+      IMPORT :: C_INT, C_PTR, ufc_mat_update_arg
+      TYPE(C_PTR), VALUE                      :: ctx
+      TYPE(ufc_mat_update_arg), INTENT(INOUT) :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_pcg_solve(ctx, b, x, mem, algo, state) BIND(C, NAME='ufc_pcg_solve')
+      IMPORT :: C_INT, C_PTR, C_DOUBLE, C_INT32_T, ufc_solver_algo, ufc_solver_state
+      TYPE(C_PTR), VALUE                    :: ctx
+      REAL(C_DOUBLE), INTENT(IN)            :: b(*)
+      REAL(C_DOUBLE), INTENT(INOUT)         :: x(*)
+      INTEGER(C_INT32_T), VALUE             :: mem
+      TYPE(ufc_solver_algo), INTENT(IN)     :: algo
+      TYPE(ufc_solver_state), INTENT(OUT)   :: state
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_pcg_solve_block(ctx, nrhs, b, x, mem, algo, states) &
+        BIND(C, NAME='ufc_pcg_solve_block')
+      IMPORT :: C_INT, C_PTR, C_DOUBLE, C_INT32_T, ufc_solver_algo, ufc_solver_state
+      TYPE(C_PTR), VALUE                    :: ctx
+      INTEGER(C_INT32_T), VALUE             :: nrhs
+      REAL(C_DOUBLE), INTENT(IN)            :: b(*)
+      REAL(C_DOUBLE), INTENT(INOUT)         :: x(*)
+      INTEGER(C_INT32_T), VALUE             :: mem
+      TYPE(ufc_solver_algo), INTENT(IN)     :: algo
+      TYPE(ufc_solver_state), INTENT(OUT)   :: states(*)
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_nr_increment(ctx, arg) BIND(C, NAME='ufc_nr_increment')
+      IMPORT :: C_INT, C_PTR, ufc_nr_arg
+      TYPE(C_PTR), VALUE               :: ctx
+      TYPE(ufc_nr_arg), INTENT(INOUT)  :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_state_commit(ctx) BIND(C, NAME='ufc_state_commit')
+      IMPORT :: C_INT, C_PTR
+      TYPE(C_PTR), VALUE :: ctx
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_state_rollback(ctx) BIND(C, NAME='ufc_state_rollback')
+      IMPORT :: C_INT, C_PTR
+      TYPE(C_PTR), VALUE :: ctx
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_get_displacement(ctx, u, mem) BIND(C, NAME='ufc_get_displacement')
+      IMPORT :: C_INT, C_PTR, C_DOUBLE, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx
+      REAL(C_DOUBLE), INTENT(OUT)   :: u(*)
+      INTEGER(C_INT32_T), VALUE     :: mem
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_adjoint_sensitivity(ctx, nrhs, u, lam, dJdE, mem) &
+        BIND(C, NAME='ufc_adjoint_sensitivity')
+      IMPORT :: C_INT, C_PTR, C_DOUBLE, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx
+      INTEGER(C_INT32_T), VALUE     :: nrhs
+      REAL(C_DOUBLE), INTENT(IN)    :: u(*), lam(*)
+      REAL(C_DOUBLE), INTENT(OUT)   :: dJdE(*)
+      INTEGER(C_INT32_T), VALUE     :: mem
+    END FUNCTION
+  END INTERFACE
+END MODULE ufc_gpu_brg

@@ -1,0 +1,178 @@
+"""Parity of the CUDA linear-elastic path with the FP64 oracle, through the C-ABI.
+
+Pattern and index work are compared bit for bit; FP64 values to 1e-12
+relative; solutions to the tolerances stated in each test.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _model(pkg, p, build=None):
+    m = pkg.FemModel.from_problem(p)
+    m.assemble(build or (pkg.BUILD_FP64 | pkg.BUILD_FP32))
+    return m
+
+
+SMALL = [
+    ("unit_cube", lambda mesh: mesh.unit_cube_uniaxial()),
+    ("box_3x2x2", lambda mesh: mesh.cantilever(3, 2, 2, 3.0, 2.0, 2.0, E=np.linspace(1e3, 5e3, 12))),
+    ("cantilever_40x8x8", lambda mesh: mesh.config1()),
+]
+
+
+@pytest.mark.parametrize("name,make", SMALL)
+def test_pattern_bit_exact(pkg, orc, name, make):
+    p = make(pkg.mesh)
+    m = pkg.FemModel.from_problem(p)
+    m.assemble(pkg.BUILD_FP64)
+    rp, col, _, _ = m.csr_export(index_base=0)
+    rp_o, col_o = orc.csr_pattern(p.n_nodes, p.conn)
+    assert np.array_equal(rp, rp_o)
+    assert np.array_equal(col, col_o)
+    rp1, col1, _, _ = m.csr_export(index_base=1)
+    assert rp1[0] == 1 and np.array_equal(rp1 - 1, rp_o) and np.array_equal(col1 - 1, col_o)
+
+
+@pytest.mark.parametrize("name,make", SMALL)
+def test_assembly_values_fp64(pkg, orc, name, make):
+    p = make(pkg.mesh)
+    m = _model(pkg, p)
+    _, _, v, _ = m.csr_export()
+    K = orc.Model(p).assemble()
+    err = np.abs(v - K.val).max() / np.abs(K.val).max()
+    assert err <= 1e-12, err
+    _, _, v32, _ = m.csr_export(values=False, values32=True)
+    err32 = np.abs(v32.astype(np.float64) - K.val).max() / np.abs(K.val).max()
+    assert err32 <= 1e-5, err32
+
+
+def test_assembly_deterministic_and_symmetric(pkg):
+    p = pkg.mesh.lognormal_cantilever(12, 6, 6, seed=7)
+    m = _model(pkg, p)
+    _, _, v1, _ = m.csr_export()
+    m.assemble(pkg.BUILD_FP64 | pkg.BUILD_FP32)
+    rp, col, v2, _ = m.csr_export()
+    assert np.array_equal(v1, v2)  # bitwise: colour-ordered scatter, no float atomics
+    n = p.n_dof
+    import scipy.sparse as sp
+
+    K = sp.csr_matrix((v2, col, rp), shape=(n, n))
+    asym = abs(K - K.T).max() / abs(K).max()
+    assert asym <= 1e-14, asym  # tests/integration/test_assembly_chain.f90:37-40
+
+
+def test_unit_cube_uniaxial(pkg):
+    # tests/ufc_core/test_c3d8_uniaxial.f90: u_x = sigma/E * L = 5e-4 (reference tolerance 1 %)
+    p = pkg.mesh.unit_cube_uniaxial()
+    m = _model(pkg, p)
+    u, st = m.solve(pkg.lifted_rhs(m, p.f), pkg.SolverAlgo(tolerance=1e-14))
+    a = p.conn[0]
+    ux = u[3 * a[[1, 2, 5, 6]]]
+    assert st.converged
+    np.testing.assert_allclose(ux, 5e-4, rtol=1e-12)
+    np.testing.assert_allclose(u[3 * a[[0, 1, 4, 5]] + 1], 0.0, atol=1e-15)  # uy on the y = 0 face
+    # lateral contraction eps_y = -nu * eps_x on the y = 1 face
+    np.testing.assert_allclose(u[3 * a[[3, 2, 6, 7]] + 1], -0.3 * 5e-4, rtol=1e-10)
+
+
+def test_spmv_and_internal_force(pkg, orc):
+    p = pkg.mesh.lognormal_cantilever(8, 4, 4, seed=3)
+    m = _model(pkg, p)
+    K = orc.Model(p).assemble()
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(p.n_dof)
+    y = m.spmv(x)
+    y_o = K.matvec(x)
+    assert np.abs(y - y_o).max() / np.abs(y_o).max() <= 1e-13
+    y32 = m.spmv(x.astype(np.float32), precision=pkg.PRECISION_FP32_REFINE)
+    assert np.abs(y32 - y_o).max() / np.abs(y_o).max() <= 1e-5
+    # matrix-free FP64 internal force equals the oracle's F_int
+    fint, r, rn, fn = m.internal_force(x)
+    f_o = orc.Model(p).fint_elastic(x)
+    assert np.abs(fint - f_o).max() / np.abs(f_o).max() <= 1e-13
+    free = pkg.mesh.free_mask(p)
+    np.testing.assert_allclose(r[free], -f_o[free], rtol=0, atol=1e-12 * np.abs(f_o).max())
+    assert np.all(r[~free] == 0.0)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32_refine"])
+def test_cantilever_40x8x8_solve(pkg, orc, prec):
+    p = pkg.mesh.config1()
+    m = pkg.FemModel.from_problem(p)
+    m.assemble(pkg.BUILD_FP64 | pkg.BUILD_FP32_ROUNDED)
+    ref = orc.Model(p)
+    u_ref, info = ref.solve_linear(rtol=1e-13)
+    mode = pkg.PRECISION_FP64 if prec == "fp64" else pkg.PRECISION_FP32_REFINE
+    b = pkg.lifted_rhs(m, p.f)
+    u, st = m.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=mode))
+    assert st.converged and st.rnorm <= 1e-10
+    if prec == "fp32_refine":
+        # this slender cantilever is too ill-conditioned for an FP32 matrix: the
+        # refined FP32 run stalls and the solve finishes in FP64 on the GPU
+        assert st.fp64_iters > 0
+    # independent FP64 residual with the oracle's matrix
+    r = b - info["K"].matvec(u)
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 2e-10
+    err = np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref)
+    assert err <= 1e-8, err
+    if prec == "fp64":
+        _, info10 = ref.solve_linear(rtol=1e-10)
+        assert abs(st.niter - info10["iters"]) <= 3, (st.niter, info10["iters"])
+
+
+def test_cantilever_beam_theory(pkg):
+    # E2E_C2_01 checks tip deflection against beam theory within 5 % (with
+    # incompatible modes); full-integration C3D8 on 40x8x8 is within 5 % of
+    # Euler-Bernoulli plus Timoshenko shear deflection.
+    p = pkg.mesh.config1()
+    m = _model(pkg, p)
+    u, st = m.solve(pkg.lifted_rhs(m, p.f), pkg.SolverAlgo(tolerance=1e-10))
+    tip = np.isclose(p.coords[:, 0], 10.0)
+    delta = -u[3 * np.nonzero(tip)[0] + 2].mean()
+    L, h, bw, P, E, nu = 10.0, 2.0, 2.0, 4.0, 210e3, 0.3
+    I = bw * h ** 3 / 12
+    G = E / (2 * (1 + nu))
+    theory = P * L ** 3 / (3 * E * I) + P * L / (5.0 / 6.0 * G * bw * h)
+    assert abs(delta - theory) / theory < 0.05, (delta, theory)
+
+
+def test_von_mises_matches_oracle(pkg, orc):
+    p = pkg.mesh.lognormal_cantilever(8, 4, 4, seed=5)
+    m = _model(pkg, p)
+    u = np.random.default_rng(1).standard_normal(p.n_dof) * 1e-3
+    sig, vm = m.stress(u)
+    sig_o, vm_o = orc.Model(p).elastic_vm(u)
+    assert np.abs(sig - sig_o).max() / np.abs(sig_o).max() <= 1e-13
+    assert np.abs(vm - vm_o).max() / np.abs(vm_o).max() <= 1e-13
+
+
+def test_not_converged_and_errors(pkg):
+    p = pkg.mesh.config1()
+    m = _model(pkg, p)
+    b = pkg.lifted_rhs(m, p.f)
+    with pytest.raises(pkg.UfcError) as ei:
+        m.solve(b, pkg.SolverAlgo(max_iter=3))
+    assert ei.value.status_code == 4  # IF_STATUS_NOT_CONVERGED
+    x, st = m.solve(b, pkg.SolverAlgo(max_iter=3), raise_on_not_converged=False)
+    assert not st.converged and st.niter == 3 and st.status == 4
+    # inverted element: Jacobian check reports IF_STATUS_ERROR, no device fault
+    q = pkg.mesh.cantilever(2, 1, 1, 2.0, 1.0, 1.0)
+    conn = q.conn.copy()
+    conn[0] = conn[0][[4, 5, 6, 7, 0, 1, 2, 3]]  # top and bottom swapped: detJ < 0
+    bad = pkg.FemModel()
+    bad.set_mesh(q.coords, conn)
+    bad.set_material(pkg.MAT_ELASTIC_ISO, q.props)
+    bad.set_bc(q.fixed)
+    bad.pattern_build()
+    with pytest.raises(pkg.UfcError) as ei:
+        bad.assemble()
+    assert ei.value.status_code == 2 and "Jacobian" in ei.value.message
+    # connectivity out of range is rejected on the host
+    with pytest.raises(pkg.UfcError) as ei:
+        bad.set_mesh(q.coords, conn + 100)
+    assert ei.value.status_code == 1
+    # the context stays usable after the failures
+    m2 = _model(pkg, pkg.mesh.unit_cube_uniaxial())
+    assert m2.solve(pkg.lifted_rhs(m2, m2.problem.f))[1].converged

@@ -1,0 +1,413 @@
+// Device-built stiffness pattern, built once per mesh.
+//
+// The canonical pattern is the block form of RT_CSR_FromTripletMerged
+// (ufc_core/L5_RT/Solver/RT_Solv_Sparse.f90:336-445): per node row, the sorted
+// unique set of nodes that share an element with it; every coupled node pair is
+// a dense 3x3 block, so the scalar CSR row 3i+r lists 3*col+c for every block
+// column col in ascending order and c = 0..2.  That canonical pattern is what
+// ufc_csr_export returns.
+//
+// Values are stored in SELL-32 form: block rows are grouped into slices of 32
+// consecutive rows, each slice padded to its longest row, and a slice's entry j
+// of all 32 rows is stored contiguously, component by component.  One warp then
+// reads 128 contiguous bytes (FP32) per load instruction in the SpMV.
+//
+// Element colouring for the deterministic scatter is the greedy colouring of
+// RT_AsmColor_Build (ufc_core/L5_RT/Assembly/RT_Asm_Color.f90:36-182), elements
+// visited in ascending order, smallest free colour first.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "c3d8_device.cuh"
+#include "ufc_internal.cuh"
+
+namespace ufc {
+
+namespace {
+
+__global__ void k_count_node_elems(int32_t E, const int32_t* __restrict__ conn, int32_t* __restrict__ cnt) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 8 * (int64_t)E) return;
+  atomicAdd(&cnt[conn[k]], 1);  // integer counts: order-independent
+}
+
+__global__ void k_fill_node_elems(int32_t E, const int32_t* __restrict__ conn, const int32_t* __restrict__ nptr,
+                                  int32_t* __restrict__ fill, int32_t* __restrict__ nlst) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 8 * (int64_t)E) return;
+  const int32_t nd = conn[k];
+  const int32_t pos = atomicAdd(&fill[nd], 1);
+  nlst[nptr[nd] + pos] = (int32_t)(k >> 3);
+}
+
+// Sort each node's element list (the fill order above is not deterministic) and
+// check the valence bound.
+__global__ void k_sort_node_elems(int32_t N, const int32_t* __restrict__ nptr, int32_t* __restrict__ nlst,
+                                  int32_t* __restrict__ err) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int32_t b = nptr[i], m = nptr[i + 1] - b;
+  if (m > kMaxValence) {
+    atomicOr(err, (int)kDevValence);
+    return;
+  }
+  for (int k = 1; k < m; ++k) {
+    const int32_t v = nlst[b + k];
+    int j = k - 1;
+    while (j >= 0 && nlst[b + j] > v) {
+      nlst[b + j + 1] = nlst[b + j];
+      --j;
+    }
+    nlst[b + j + 1] = v;
+  }
+}
+
+// Sorted unique neighbours of node i into buf (capacity kMaxRowBlocks); returns
+// the count, or -1 when it would exceed the capacity.
+__device__ int node_neighbours(int64_t i, const int32_t* __restrict__ conn, const int32_t* __restrict__ nptr,
+                               const int32_t* __restrict__ nlst, int32_t* buf) {
+  int u = 0;
+  for (int32_t k = nptr[i]; k < nptr[i + 1]; ++k) {
+    const int64_t e = nlst[k];
+    for (int a = 0; a < 8; ++a) {
+      const int32_t v = conn[e * 8 + a];
+      int lo = 0, hi = u;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (buf[mid] < v) lo = mid + 1;
+        else hi = mid;
+      }
+      if (lo < u && buf[lo] == v) continue;
+      if (u == kMaxRowBlocks) return -1;
+      for (int j = u; j > lo; --j) buf[j] = buf[j - 1];
+      buf[lo] = v;
+      ++u;
+    }
+  }
+  return u;
+}
+
+__global__ void k_row_count(int32_t N, const int32_t* __restrict__ conn, const int32_t* __restrict__ nptr,
+                            const int32_t* __restrict__ nlst, int32_t* __restrict__ cnt, int32_t* __restrict__ err) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int32_t buf[kMaxRowBlocks];
+  const int u = node_neighbours(i, conn, nptr, nlst, buf);
+  if (u < 0) atomicOr(err, (int)kDevRowBlocks);
+  cnt[i] = u < 0 ? 0 : u;
+}
+
+__global__ void k_row_fill(int32_t N, const int32_t* __restrict__ conn, const int32_t* __restrict__ nptr,
+                           const int32_t* __restrict__ nlst, const int32_t* __restrict__ brow,
+                           int32_t* __restrict__ bcol) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int32_t buf[kMaxRowBlocks];
+  const int u = node_neighbours(i, conn, nptr, nlst, buf);
+  for (int k = 0; k < u; ++k) bcol[brow[i] + k] = buf[k];
+}
+
+// Longest row of each slice, in blocks.
+__global__ void k_slice_len(int32_t N, int64_t nslices, const int32_t* __restrict__ brow, int64_t* __restrict__ len) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslices) return;
+  int32_t m = 0;
+  for (int t = 0; t < kSlice; ++t) {
+    const int64_t r = s * kSlice + t;
+    if (r < N) m = max(m, brow[r + 1] - brow[r]);
+  }
+  len[s] = (int64_t)m * kSlice;
+}
+
+// SELL column array: real entries, then padding that points at the row itself
+// (zero values), one thread per padded row.
+__global__ void k_sell_fill(int32_t N, int64_t nslices, const int32_t* __restrict__ brow,
+                            const int32_t* __restrict__ bcol, const int64_t* __restrict__ sptr,
+                            int32_t* __restrict__ scol, int32_t* __restrict__ dpos) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nslices * kSlice) return;
+  const int64_t s = r / kSlice, t = r % kSlice;
+  const int64_t base = sptr[s], len = (sptr[s + 1] - base) / kSlice;
+  const int32_t b = r < N ? brow[r] : 0, m = r < N ? brow[r + 1] - b : 0;
+  const int32_t self = r < N ? (int32_t)r : 0;
+  for (int64_t j = 0; j < len; ++j) {
+    const int32_t cj = j < m ? bcol[b + j] : self;
+    scol[base + j * kSlice + t] = cj;
+    if (r < N && j < m && cj == r) dpos[r] = (int32_t)(base + j * kSlice + t);
+  }
+}
+
+// slot[e][a][b] = SELL position of block (conn[a], conn[b]).
+__global__ void k_slots(int32_t E, const int32_t* __restrict__ conn, const int32_t* __restrict__ brow,
+                        const int32_t* __restrict__ bcol, const int64_t* __restrict__ sptr,
+                        int32_t* __restrict__ slot, int32_t* __restrict__ err) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 8 * (int64_t)E) return;
+  const int64_t e = k >> 3;
+  const int a = (int)(k & 7);
+  const int32_t r = conn[e * 8 + a];
+  const int64_t s = r / kSlice, t = r % kSlice;
+  for (int b = 0; b < 8; ++b) {
+    const int32_t cb = conn[e * 8 + b];
+    int lo = brow[r], hi = brow[r + 1] - 1, found = -1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      const int32_t v = bcol[mid];
+      if (v < cb) lo = mid + 1;
+      else if (v > cb) hi = mid - 1;
+      else {
+        found = mid - brow[r];
+        break;
+      }
+    }
+    if (found < 0) {
+      atomicOr(err, (int)kDevPattern);
+      found = 0;
+    }
+    slot[e * 64 + a * 8 + b] = (int32_t)(sptr[s] + (int64_t)found * kSlice + t);
+  }
+}
+
+// Scalar CSR export from the block pattern, one thread per (block row, entry).
+template <typename TV>
+__global__ void k_export(int32_t N, const int32_t* __restrict__ brow, const int32_t* __restrict__ bcol,
+                         const int64_t* __restrict__ sptr, const TV* __restrict__ val, int base,
+                         int64_t* __restrict__ row_ptr, int32_t* __restrict__ col, double* __restrict__ v64,
+                         float* __restrict__ v32) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int64_t b = brow[i], m = brow[i + 1] - b;
+  if (row_ptr) {
+    for (int r = 0; r < 3; ++r) row_ptr[3 * i + r] = 9 * b + r * 3 * m + base;
+    if (i == N - 1) row_ptr[3 * (int64_t)N] = 9 * (int64_t)brow[N] + base;
+  }
+  const int64_t s = i / kSlice, t = i % kSlice;
+  for (int64_t k = 0; k < m; ++k) {
+    const int64_t P = sptr[s] + k * kSlice + t;
+    const int32_t cb = bcol[b + k];
+    for (int r = 0; r < 3; ++r) {
+      const int64_t o = 9 * b + r * 3 * m + 3 * k;
+      for (int cc = 0; cc < 3; ++cc) {
+        if (col) col[o + cc] = 3 * cb + cc + base;
+        if (val) {
+          const TV x = val[vpos(P, r * 3 + cc)];
+          if (v64) v64[o + cc] = (double)x;
+          if (v32) v32[o + cc] = (float)x;
+        }
+      }
+    }
+  }
+}
+
+// Greedy colouring on the host (deterministic, visits elements in order).
+int color_elements(Ctx* c, std::vector<int32_t>& color) {
+  const int32_t N = c->N, E = c->E;
+  const std::vector<int32_t>& conn = c->h_conn;
+  std::vector<int32_t> nptr(N + 1, 0), nlst((size_t)E * 8);
+  for (int64_t k = 0; k < 8 * (int64_t)E; ++k) nptr[conn[k] + 1]++;
+  for (int32_t i = 0; i < N; ++i) nptr[i + 1] += nptr[i];
+  {
+    std::vector<int32_t> fill(nptr.begin(), nptr.end() - 1);
+    for (int64_t k = 0; k < 8 * (int64_t)E; ++k) nlst[fill[conn[k]]++] = (int32_t)(k >> 3);
+  }
+  color.assign(E, -1);
+  int ncol = 0;
+  for (int64_t e = 0; e < E; ++e) {
+    uint64_t used[4] = {0, 0, 0, 0};
+    for (int a = 0; a < 8; ++a) {
+      const int32_t nd = conn[e * 8 + a];
+      for (int32_t k = nptr[nd]; k < nptr[nd + 1]; ++k) {
+        const int32_t f = nlst[k];
+        if (f < e) used[color[f] >> 6] |= 1ull << (color[f] & 63);
+      }
+    }
+    int col = 0;
+    while (col < 256 && ((used[col >> 6] >> (col & 63)) & 1ull)) ++col;
+    if (col >= 256) return fail(c, UFC_STATUS_UNSUPPORTED, "element colouring needs more than 256 colours");
+    color[e] = col;
+    ncol = std::max(ncol, col + 1);
+  }
+  c->ncol = ncol;
+  return UFC_STATUS_OK;
+}
+
+template <class T>
+int scan_exclusive(Ctx* c, const T* in, T* out, int64_t n) {
+  size_t bytes = 0;
+  UFC_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, c->stream));
+  void* tmp = nullptr;
+  UFC_CUDA(c, cudaMallocAsync(&tmp, bytes, c->stream));
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, c->stream);
+  cudaFreeAsync(tmp, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cub::DeviceScan::ExclusiveSum");
+  return UFC_STATUS_OK;
+}
+
+}  // namespace
+
+int build_pattern(Ctx* c) {
+  if (c->E <= 0 || c->N <= 0) return fail(c, UFC_STATUS_INVALID, "ufc_pattern_build: mesh not set");
+  release_graphs(c);
+  const int32_t N = c->N, E = c->E;
+
+  // 1. colouring (host) and colour-grouped element lists
+  std::vector<int32_t> color;
+  UFC_TRY(color_elements(c, color));
+  c->col_off.assign(c->ncol + 1, 0);
+  for (int32_t e = 0; e < E; ++e) c->col_off[color[e] + 1]++;
+  for (int k = 0; k < c->ncol; ++k) c->col_off[k + 1] += c->col_off[k];
+  {
+    std::vector<int32_t> lst(E), fill(c->col_off.begin(), c->col_off.end() - 1);
+    for (int32_t e = 0; e < E; ++e) lst[fill[color[e]]++] = e;
+    UFC_TRY(dalloc(c, &c->col_elems, E));
+    UFC_CUDA(c, cudaMemcpyAsync(c->col_elems, lst.data(), sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream));
+    UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+
+  // 2. node -> element adjacency on the device
+  int32_t *cnt = nullptr, *nptr = nullptr, *fill = nullptr, *nlst = nullptr;
+  UFC_TRY(dalloc(c, &cnt, (int64_t)N + 1));
+  UFC_TRY(dalloc(c, &nptr, (int64_t)N + 1));
+  UFC_TRY(dalloc(c, &fill, N));
+  UFC_TRY(dalloc(c, &nlst, 8 * (int64_t)E));
+  UFC_CUDA(c, cudaMemsetAsync(cnt, 0, sizeof(int32_t) * ((size_t)N + 1), c->stream));
+  UFC_CUDA(c, cudaMemsetAsync(fill, 0, sizeof(int32_t) * N, c->stream));
+  UFC_CUDA(c, cudaMemsetAsync(c->dev_err, 0, sizeof(int32_t), c->stream));
+  k_count_node_elems<<<grid_for(8 * (int64_t)E, 256), 256, 0, c->stream>>>(E, c->conn, cnt);
+  UFC_TRY(scan_exclusive(c, cnt, nptr, (int64_t)N + 1));
+  k_fill_node_elems<<<grid_for(8 * (int64_t)E, 256), 256, 0, c->stream>>>(E, c->conn, nptr, fill, nlst);
+  k_sort_node_elems<<<grid_for(N, 128), 128, 0, c->stream>>>(N, nptr, nlst, c->dev_err);
+  UFC_CUDA(c, cudaGetLastError());
+  int st = check_dev_err(c, "ufc_pattern_build (node adjacency)");
+  if (st != UFC_STATUS_OK) {
+    dfree(&cnt); dfree(&nptr); dfree(&fill); dfree(&nlst);
+    return st;
+  }
+
+  // 3. block rows: count, scan, fill
+  UFC_TRY(dalloc(c, &c->brow, (int64_t)N + 1));
+  UFC_CUDA(c, cudaMemsetAsync(cnt, 0, sizeof(int32_t) * ((size_t)N + 1), c->stream));
+  k_row_count<<<grid_for(N, 128), 128, 0, c->stream>>>(N, c->conn, nptr, nlst, cnt, c->dev_err);
+  UFC_TRY(scan_exclusive(c, cnt, c->brow, (int64_t)N + 1));
+  st = check_dev_err(c, "ufc_pattern_build (row count)");
+  if (st != UFC_STATUS_OK) {
+    dfree(&cnt); dfree(&nptr); dfree(&fill); dfree(&nlst);
+    return st;
+  }
+  int32_t nnzb = 0;
+  UFC_CUDA(c, cudaMemcpyAsync(&nnzb, c->brow + N, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->nnzb = nnzb;
+  UFC_TRY(dalloc(c, &c->bcol, nnzb));
+  k_row_fill<<<grid_for(N, 128), 128, 0, c->stream>>>(N, c->conn, nptr, nlst, c->brow, c->bcol);
+  UFC_CUDA(c, cudaGetLastError());
+  {
+    std::vector<int32_t> h(N + 1);
+    UFC_CUDA(c, cudaMemcpyAsync(h.data(), c->brow, sizeof(int32_t) * (N + 1), cudaMemcpyDeviceToHost, c->stream));
+    UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+    int32_t m = 0;
+    for (int32_t i = 0; i < N; ++i) m = std::max(m, h[i + 1] - h[i]);
+    c->max_row_blocks = m;
+  }
+
+  // 4. SELL-32 layout
+  c->nslices = (N + kSlice - 1) / kSlice;
+  int64_t* slen = nullptr;
+  UFC_TRY(dalloc(c, &slen, c->nslices + 1));
+  UFC_CUDA(c, cudaMemsetAsync(slen, 0, sizeof(int64_t) * (c->nslices + 1), c->stream));
+  k_slice_len<<<grid_for(c->nslices, 256), 256, 0, c->stream>>>(N, c->nslices, c->brow, slen);
+  UFC_TRY(dalloc(c, &c->slice_ptr, c->nslices + 1));
+  UFC_TRY(scan_exclusive(c, slen, c->slice_ptr, c->nslices + 1));
+  UFC_CUDA(c, cudaMemcpyAsync(&c->sell_blocks, c->slice_ptr + c->nslices, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                              c->stream));
+  UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  dfree(&slen);
+  if (c->sell_blocks >= (int64_t)1 << 31)
+    return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pattern_build: more than 2^31 stored blocks");
+  UFC_TRY(dalloc(c, &c->sell_col, c->sell_blocks));
+  UFC_TRY(dalloc(c, &c->dpos, N));
+  k_sell_fill<<<grid_for(c->nslices * kSlice, 128), 128, 0, c->stream>>>(N, c->nslices, c->brow, c->bcol,
+                                                                         c->slice_ptr, c->sell_col, c->dpos);
+  UFC_TRY(dalloc(c, &c->slot, 64 * (int64_t)E));
+  k_slots<<<grid_for(8 * (int64_t)E, 128), 128, 0, c->stream>>>(E, c->conn, c->brow, c->bcol, c->slice_ptr, c->slot,
+                                                                c->dev_err);
+  UFC_CUDA(c, cudaGetLastError());
+  st = check_dev_err(c, "ufc_pattern_build (slots)");
+  dfree(&cnt); dfree(&nptr); dfree(&fill); dfree(&nlst);
+  if (st != UFC_STATUS_OK) return st;
+
+  // grid reductions keep 4 partial sums per block; the SpMV grid has one
+  // thread per (padded) block row
+  const int64_t need = 4 * std::max<int64_t>((c->nslices * kSlice + 255) / 256, 65536);
+  if (need > c->partials_cap) {
+    UFC_TRY(dalloc(c, &c->partials, need));
+    c->partials_cap = need;
+  }
+
+  // values are (re)allocated on the next assembly
+  dfree(&c->val64);
+  dfree(&c->val32);
+  c->has_val64 = c->has_val32 = false;
+  c->has_pattern = true;
+  return UFC_STATUS_OK;
+}
+
+int export_csr(Ctx* c, const ufc_csr_export_arg* a) {
+  if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_csr_export: pattern not built");
+  if (a->index_base != 0 && a->index_base != 1) return fail(c, UFC_STATUS_INVALID, "ufc_csr_export: index_base");
+  if ((a->values && !c->has_val64 && !c->has_val32) || (a->values32 && !c->has_val32 && !c->has_val64))
+    return fail(c, UFC_STATUS_INVALID, "ufc_csr_export: no assembled values");
+  const int64_t nnz = 9 * c->nnzb;
+  const bool dev = a->mem == UFC_MEM_DEVICE;
+  int64_t* rp = a->row_ptr;
+  int32_t* col = a->col_ind;
+  double* v64 = a->values;
+  float* v32 = a->values32;
+  int64_t* d_rp = nullptr;
+  int32_t* d_col = nullptr;
+  double* d_v64 = nullptr;
+  float* d_v32 = nullptr;
+  if (!dev) {
+    if (rp) UFC_TRY(dalloc(c, &d_rp, c->n + 1));
+    if (col) UFC_TRY(dalloc(c, &d_col, nnz));
+    if (v64) UFC_TRY(dalloc(c, &d_v64, nnz));
+    if (v32) UFC_TRY(dalloc(c, &d_v32, nnz));
+  } else {
+    d_rp = rp; d_col = col; d_v64 = v64; d_v32 = v32;
+  }
+  const int g = grid_for(c->N, 128);
+  // FP64 export reads the FP64 values; FP32 export reads the FP32 values when present.
+  if (d_rp || d_col || d_v64) {
+    if (c->has_val64 || !d_v64)
+      k_export<double><<<g, 128, 0, c->stream>>>(c->N, c->brow, c->bcol, c->slice_ptr, d_v64 ? c->val64 : nullptr,
+                                                 a->index_base, d_rp, d_col, d_v64, nullptr);
+    else
+      k_export<float><<<g, 128, 0, c->stream>>>(c->N, c->brow, c->bcol, c->slice_ptr, c->val32, a->index_base, d_rp,
+                                                d_col, d_v64, nullptr);
+  }
+  if (d_v32) {
+    // difference-form FP32 values hold row sums on the diagonal: export the
+    // standard form, rounded from FP64, instead
+    if (c->has_val32 && !(c->val32_diff && c->has_val64))
+      k_export<float><<<g, 128, 0, c->stream>>>(c->N, c->brow, c->bcol, c->slice_ptr, c->val32, a->index_base,
+                                                nullptr, nullptr, nullptr, d_v32);
+    else
+      k_export<double><<<g, 128, 0, c->stream>>>(c->N, c->brow, c->bcol, c->slice_ptr, c->val64, a->index_base,
+                                                 nullptr, nullptr, nullptr, d_v32);
+  }
+  UFC_CUDA(c, cudaGetLastError());
+  if (!dev) {
+    if (rp) UFC_CUDA(c, cudaMemcpyAsync(rp, d_rp, sizeof(int64_t) * (c->n + 1), cudaMemcpyDeviceToHost, c->stream));
+    if (col) UFC_CUDA(c, cudaMemcpyAsync(col, d_col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, c->stream));
+    if (v64) UFC_CUDA(c, cudaMemcpyAsync(v64, d_v64, sizeof(double) * nnz, cudaMemcpyDeviceToHost, c->stream));
+    if (v32) UFC_CUDA(c, cudaMemcpyAsync(v32, d_v32, sizeof(float) * nnz, cudaMemcpyDeviceToHost, c->stream));
+    UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+    dfree(&d_rp); dfree(&d_col); dfree(&d_v64); dfree(&d_v32);
+  }
+  return UFC_STATUS_OK;
+}
+
+}  // namespace ufc

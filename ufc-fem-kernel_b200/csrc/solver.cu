@@ -1,0 +1,640 @@
+// SELL-32 SpMV and the Jacobi-preconditioned CG of NM_Solver_PCG /
+// iter_pcg (ufc_core/L2_NM/Solver/NM_Solv_Core.f90:363-423,
+// ufc_core/L2_NM/Solver/LinSolv/NM_Solv_IterSolver.f90:713-846).
+//
+// One CG iteration is three kernels:
+//   k_spmv<.., kCg>   q = K p, fused p.q, alpha = r.z / p.q
+//   k_cg_update       x += alpha p (x in FP64), r -= alpha q, z = D^-1 r fused,
+//                     r.z and r.r, beta, the stop test and the refinement trigger
+//   k_cg_pupdate      p = D^-1 r + beta p
+// The scalars live in device memory (CgScalars) and every kernel returns at
+// once when the run has stopped, so batches of iterations are launched as one
+// CUDA graph and the host only looks at the scalars between batches.
+//
+// UFC_PRECISION_FP32_REFINE keeps the matrix and the CG vectors in FP32 and the
+// solution in FP64.  Whenever the FP32 recursive residual has fallen by
+// refine_delta since the last replacement, and whenever it meets the tolerance,
+// the residual is recomputed in FP64 as r = b - K x with the FP64 element
+// operator (matrix-free, K assembled from FP64 element stiffnesses) and
+// replaces the recursive one (residual replacement).  The run ends when the
+// FP64 residual meets the tolerance.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "c3d8_device.cuh"
+#include "reduce.cuh"
+#include "ufc_internal.cuh"
+
+namespace ufc {
+
+int apply_fp64_eliminated(Ctx* c, const double* x, double* y);
+
+namespace {
+
+constexpr int kSpmvBlock = 256;
+constexpr int kVecBlock = 256;
+
+int vec_grid(int64_t n) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t need = (n + kVecBlock - 1) / kVecBlock;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * 8));
+}
+
+enum SpmvMode { kPlain = 0, kCg = 1 };
+
+// y = K x, one thread per block row of a SELL-32 slice (a warp = a slice).
+// TV: stored value type, TX: vector type, TA: accumulator type of the row sums.
+// DIFF: values in difference form (diagonal slot = block row sum S_i), so the
+// row is evaluated as sum_{j != i} K_ij (x_j - x_i) + S_i x_i.
+template <typename TV, typename TX, typename TA, int MODE, bool DIFF>
+__global__ void __launch_bounds__(kSpmvBlock)
+    k_spmv(int32_t N, int64_t nrows_pad, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
+           const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y, CgScalars* __restrict__ scal,
+           double* __restrict__ partials) {
+  if (MODE == kCg && scal->stop) return;
+  const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
+  double dot[1] = {0.0};
+  if (row < nrows_pad) {
+    const int64_t s = row >> 5;
+    const int t = (int)(row & 31);
+    const int64_t base = sptr[s];
+    const int len = (int)((sptr[s + 1] - base) >> 5);
+    const int32_t* cp = col + base + t;
+    const TV* vp = val + 9 * base + t;
+    TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
+    TA xi0 = TA(0), xi1 = TA(0), xi2 = TA(0);
+    if (DIFF && row < N) {
+      xi0 = (TA)x[3 * row];
+      xi1 = (TA)x[3 * row + 1];
+      xi2 = (TA)x[3 * row + 2];
+    }
+#pragma unroll 2
+    for (int j = 0; j < len; ++j) {
+      const int64_t cj = __ldcs(cp + 32 * j);
+      TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
+      if (DIFF && cj != row) {
+        x0 -= xi0;
+        x1 -= xi1;
+        x2 -= xi2;
+      }
+      const TV* v = vp + 288 * (int64_t)j;
+      a0 += (TA)__ldcs(v) * x0 + (TA)__ldcs(v + 32) * x1 + (TA)__ldcs(v + 64) * x2;
+      a1 += (TA)__ldcs(v + 96) * x0 + (TA)__ldcs(v + 128) * x1 + (TA)__ldcs(v + 160) * x2;
+      a2 += (TA)__ldcs(v + 192) * x0 + (TA)__ldcs(v + 224) * x1 + (TA)__ldcs(v + 256) * x2;
+    }
+    if (row < N) {
+      y[3 * row] = (TX)a0;
+      y[3 * row + 1] = (TX)a1;
+      y[3 * row + 2] = (TX)a2;
+      if (MODE == kCg)
+        dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
+    }
+  }
+  if (MODE == kCg) {
+    double tot[1];
+    if (grid_sum<1>(dot, partials, &scal->ticket[0], tot)) {
+      scal->pq = tot[0];
+      if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
+        scal->stop = 3;
+      } else {
+        scal->alpha = scal->rz / tot[0];
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecBlock)
+    k_cg_update(int64_t n, const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ r,
+                double* __restrict__ x, const T* __restrict__ dinv, CgScalars* __restrict__ scal,
+                double* __restrict__ partials) {
+  if (scal->stop) return;
+  const double alpha = scal->alpha;
+  const T a = (T)alpha;
+  T rz = T(0), rr = T(0);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T pi = p[i], qi = q[i];
+    x[i] += alpha * (double)pi;
+    const T ri = r[i] - a * qi;
+    r[i] = ri;
+    const T zi = dinv ? dinv[i] * ri : ri;
+    rz += ri * zi;
+    rr += ri * ri;
+  }
+  double v[2] = {(double)rz, (double)rr}, tot[2];
+  if (grid_sum<2>(v, partials, &scal->ticket[1], tot)) {
+    const double rz_old = scal->rz;
+    scal->rz_old = rz_old;
+    scal->rz = tot[0];
+    scal->rr = tot[1];
+    scal->beta = tot[0] / rz_old;
+    const int it = scal->iter + 1;
+    scal->iter = it;
+    if (tot[1] <= scal->tol2) scal->stop = 1;
+    else if (!(fabs(rz_old) > 1e-300) || !isfinite(tot[0])) scal->stop = 3;
+    else if (it >= scal->max_iter) scal->stop = 2;
+    if (scal->delta2 > 0.0 && tot[1] < scal->delta2 * scal->rr_ref) scal->want_update = 1;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecBlock)
+    k_cg_pupdate(int64_t n, const T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ p,
+                 const CgScalars* __restrict__ scal) {
+  if (scal->stop) return;
+  const T beta = (T)scal->beta;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T ri = r[i];
+    p[i] = (dinv ? dinv[i] * ri : ri) + beta * p[i];
+  }
+}
+
+// res = b - y and ||res||^2 -> scal->true_rr (and ||b||^2 -> scal->bb when asked).
+__global__ void __launch_bounds__(kVecBlock)
+    k_resid(int64_t n, const double* __restrict__ b, const double* y, double* res,
+            CgScalars* __restrict__ scal, double* __restrict__ partials, int want_bb) {
+  double rr = 0.0, bb = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double bi = b[i];
+    const double ri = bi - (y ? y[i] : 0.0);
+    res[i] = ri;
+    rr += ri * ri;
+    bb += bi * bi;
+  }
+  double v[2] = {rr, bb}, tot[2];
+  if (grid_sum<2>(v, partials, &scal->ticket[2], tot)) {
+    scal->true_rr = tot[0];
+    if (want_bb) scal->bb = tot[1];
+  }
+}
+
+// Residual replacement: r := res (rounded to T), z = D^-1 r, r.z and r.r.
+// mode 0: mid-run (p already updated); 1: the run stopped before its p update,
+// which is then done with beta = r.z / rz_old; 2: start (beta = 0, p = z).
+template <typename T>
+__global__ void __launch_bounds__(kVecBlock)
+    k_replace(int64_t n, const double* __restrict__ res, T* __restrict__ r, const T* __restrict__ dinv,
+              CgScalars* __restrict__ scal, double* __restrict__ partials, int mode) {
+  T rz = T(0), rr = T(0);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T ri = (T)res[i];
+    r[i] = ri;
+    const T zi = dinv ? dinv[i] * ri : ri;
+    rz += ri * zi;
+    rr += ri * ri;
+  }
+  double v[2] = {(double)rz, (double)rr}, tot[2];
+  if (grid_sum<2>(v, partials, &scal->ticket[3], tot)) {
+    if (mode == 1) scal->beta = tot[0] / scal->rz_old;
+    if (mode == 2) scal->beta = 0.0;
+    scal->rz = tot[0];
+    scal->rr = tot[1];
+    scal->rr_ref = tot[1];
+    scal->stop = 0;
+    scal->want_update = 0;
+  }
+}
+
+template <typename T>
+__global__ void k_zero(int64_t n, T* __restrict__ v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = T(0);
+}
+
+struct Run {
+  Ctx* c;
+  int prec;  // UFC_PRECISION_*
+  int64_t n;
+  int vg;    // vector-kernel grid
+  int sg;    // SpMV grid
+};
+
+// CG vectors of type TX over stored values of type TV.
+template <typename TV, typename TX>
+struct Vecs {
+  TX *r, *p, *q;
+  const TV* val;
+  const TX* dinv;
+};
+
+template <typename TV, typename TX>
+Vecs<TV, TX> vecs(Ctx* c, bool precond) {
+  Vecs<TV, TX> v;
+  if constexpr (sizeof(TX) == 8) {
+    v.r = c->r64; v.p = c->p64; v.q = c->q64;
+    v.dinv = precond ? c->dinv64 : nullptr;
+  } else {
+    v.r = c->r32; v.p = c->p32; v.q = c->q32;
+    v.dinv = precond ? c->dinv32 : nullptr;
+  }
+  if constexpr (sizeof(TV) == 8) v.val = c->val64;
+  else v.val = c->val32;
+  return v;
+}
+
+template <typename TV, typename TX, typename TA>
+void launch_iteration(const Run& R, const Vecs<TV, TX>& V, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
+  Ctx* c = R.c;
+  if (ev0) cudaEventRecord(ev0, st);
+  if (sizeof(TV) == 4 && c->val32_diff)
+    k_spmv<TV, TX, TA, kCg, true><<<R.sg, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col,
+                                                               V.val, V.p, V.q, c->scal, c->partials);
+  else
+    k_spmv<TV, TX, TA, kCg, false><<<R.sg, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col,
+                                                                V.val, V.p, V.q, c->scal, c->partials);
+  if (ev1) cudaEventRecord(ev1, st);
+  k_cg_update<TX><<<R.vg, kVecBlock, 0, st>>>(R.n, V.p, V.q, V.r, c->x64, V.dinv, c->scal, c->partials);
+  k_cg_pupdate<TX><<<R.vg, kVecBlock, 0, st>>>(R.n, V.r, V.dinv, V.p, c->scal);
+  c->launches += 3;
+}
+
+// FP64 residual of the current x64 into y64 / r-source, true_rr on the device.
+int true_residual(const Run& R, bool want_bb) {
+  Ctx* c = R.c;
+  if (R.prec == UFC_PRECISION_FP64) {
+    k_spmv<double, double, double, kPlain, false><<<R.sg, kSpmvBlock, 0, c->stream>>>(
+        c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col, c->val64, c->x64, c->y64, nullptr, nullptr);
+    UFC_CUDA(c, cudaGetLastError());
+    c->launches += 1;
+  } else {
+    UFC_TRY(apply_fp64_eliminated(c, c->x64, c->y64));
+  }
+  k_resid<<<R.vg, kVecBlock, 0, c->stream>>>(R.n, c->b64, c->y64, c->y64, c->scal, c->partials, want_bb ? 1 : 0);
+  UFC_CUDA(c, cudaGetLastError());
+  c->launches += 1;
+  return UFC_STATUS_OK;
+}
+
+template <typename TV, typename TX>
+int replace(const Run& R, const Vecs<TV, TX>& V, int mode) {
+  Ctx* c = R.c;
+  k_replace<TX><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, c->y64, V.r, V.dinv, c->scal, c->partials, mode);
+  UFC_CUDA(c, cudaGetLastError());
+  c->launches += 1;
+  if (mode != 0) {
+    k_cg_pupdate<TX><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, V.r, V.dinv, V.p, c->scal);
+    UFC_CUDA(c, cudaGetLastError());
+    c->launches += 1;
+  }
+  return UFC_STATUS_OK;
+}
+
+int read_scalars(Ctx* c) {
+  UFC_CUDA(c, cudaMemcpyAsync(c->h_scal, c->scal, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->stream));
+  UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  return UFC_STATUS_OK;
+}
+
+template <typename TV, typename TX, typename TA>
+int get_graph(const Run& R, const Vecs<TV, TX>& V, int batch, cudaGraphExec_t* out) {
+  Ctx* c = R.c;
+  // one cached graph per (value, vector, accumulator) type combination
+  const int slot = sizeof(TV) == 8 ? 0 : sizeof(TX) == 8 ? 3 : sizeof(TA) == 8 ? 2 : 1;
+  const void* key = (const void*)V.dinv;  // graphs are rebuilt when buffers or the preconditioner change
+  if (c->cg_graph[slot] && c->cg_graph_batch[slot] == batch && c->cg_graph_key[slot] == key) {
+    *out = c->cg_graph[slot];
+    return UFC_STATUS_OK;
+  }
+  if (c->cg_graph[slot]) cudaGraphExecDestroy(c->cg_graph[slot]);
+  c->cg_graph[slot] = nullptr;
+  cudaGraph_t g;
+  const int64_t counted = c->launches;  // captured launches run only when the graph is launched
+  UFC_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < batch; ++k) launch_iteration<TV, TX, TA>(R, V, c->stream, nullptr, nullptr);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  c->launches = counted;
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&c->cg_graph[slot], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+  c->cg_graph_batch[slot] = batch;
+  c->cg_graph_key[slot] = key;
+  *out = c->cg_graph[slot];
+  return UFC_STATUS_OK;
+}
+
+int ensure_vectors(Ctx* c, int prec) {
+  const int64_t n = c->n;
+  bool realloc = false;
+  auto need = [&](auto** p) -> int {
+    if (*p) return UFC_STATUS_OK;
+    realloc = true;
+    return dalloc(c, p, n);
+  };
+  UFC_TRY(need(&c->x64));
+  UFC_TRY(need(&c->b64));
+  UFC_TRY(need(&c->y64));
+  if (prec == UFC_PRECISION_FP64 || prec == UFC_PRECISION_FP32_MATRIX) {
+    UFC_TRY(need(&c->r64));
+    UFC_TRY(need(&c->p64));
+    UFC_TRY(need(&c->q64));
+  } else {
+    UFC_TRY(need(&c->r32));
+    UFC_TRY(need(&c->p32));
+    UFC_TRY(need(&c->q32));
+  }
+  if (prec != UFC_PRECISION_FP64) UFC_TRY(need(&c->xb64));
+  if (realloc) release_graphs(c);
+  return UFC_STATUS_OK;
+}
+
+template <typename TV, typename TX, typename TA>
+int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
+  const int prec = algo->precision_mode;
+  Run R{c, prec, c->n, vec_grid(c->n), (int)((c->nslices * kSlice + kSpmvBlock - 1) / kSpmvBlock)};
+  const bool precond = algo->precond_type == UFC_SOLV_PREC_JACOBI;
+  Vecs<TV, TX> V = vecs<TV, TX>(c, precond);
+  const int batch = algo->check_every > 0 ? algo->check_every : 32;
+
+  cudaEvent_t t0, t1;
+  UFC_CUDA(c, cudaEventCreate(&t0));
+  UFC_CUDA(c, cudaEventCreate(&t1));
+  UFC_CUDA(c, cudaEventRecord(t0, c->stream));
+  c->timing = ufc_timing_info{};
+  c->timing.precision = prec;
+  c->timing.spmv_bytes = spmv_bytes(c, prec);
+  c->launches = 0;
+
+  // scalars: reset and configure
+  CgScalars h{};
+  h.max_iter = algo->max_iter > 0 ? algo->max_iter : 1;
+  h.delta2 = 0.0;
+  if (prec != UFC_PRECISION_FP64) {
+    const double d = algo->refine_delta > 0.0 ? algo->refine_delta : 0.1;
+    h.delta2 = d * d;
+  }
+  UFC_CUDA(c, cudaMemcpyAsync(c->scal, &h, sizeof(CgScalars), cudaMemcpyHostToDevice, c->stream));
+  UFC_TRY(true_residual(R, true));
+  UFC_TRY(read_scalars(c));
+  const double bnorm_raw = std::sqrt(c->h_scal->bb);
+  const double bnorm = bnorm_raw < 1e-30 ? 1.0 : bnorm_raw;
+  const double tol = std::max(algo->tolerance * bnorm, algo->abs_tolerance);
+  st->initial_residual = std::sqrt(c->h_scal->true_rr);
+  double true_rr = c->h_scal->true_rr;
+  int flag = 0;
+  bool converged = std::sqrt(true_rr) <= tol;
+  int n_refine = 0;
+
+  if (!converged) {
+    double tol2 = tol * tol;
+    UFC_CUDA(c, cudaMemcpyAsync(&c->scal->tol2, &tol2, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    UFC_TRY(replace(R, V, 2));
+    cudaGraphExec_t graph = nullptr;
+    if (!c->instrument) UFC_TRY((get_graph<TV, TX, TA>(R, V, batch, &graph)));
+    std::vector<cudaEvent_t> evs;
+    if (c->instrument) {
+      evs.resize(2 * batch);
+      for (auto& e : evs) UFC_CUDA(c, cudaEventCreate(&e));
+    }
+    CgScalars* hs[2] = {c->h_scal + 1, c->h_scal + 2};
+    cudaEvent_t done[2];
+    UFC_CUDA(c, cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+    UFC_CUDA(c, cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+    int slot = 0, in_flight = 0, iter_seen = 0;
+    int stall = 0, restarts = 0;
+    double best_rr = true_rr;
+    constexpr int kMaxStall = 12;      // replacements without a 4x drop of ||b - K x||^2
+    constexpr int kMaxRestarts = 4;    // restarts after a breakdown of the recurrence
+    constexpr double kDiverge = 1e4;   // ||b - K x|| grew 100x above the best seen
+    const bool keep_best = c->xb64 != nullptr;
+    if (keep_best) cudaMemcpyAsync(c->xb64, c->x64, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream);
+    bool finished = false;
+    int status = UFC_STATUS_OK;
+    while (!finished) {
+      if (graph) {
+        cudaError_t e = cudaGraphLaunch(graph, c->stream);
+        if (e != cudaSuccess) {
+          status = cuda_fail(c, e, "cudaGraphLaunch");
+          break;
+        }
+        c->launches += 3 * (int64_t)batch;
+      } else {
+        for (int k = 0; k < batch; ++k)
+          launch_iteration<TV, TX, TA>(R, V, c->stream, evs[2 * k], evs[2 * k + 1]);
+      }
+      cudaMemcpyAsync(hs[slot], c->scal, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->stream);
+      cudaEventRecord(done[slot], c->stream);
+      if (c->instrument) {
+        // one batch in flight at a time: the events are reused; only the
+        // launches that did an iteration (not the no-op tail) are counted
+        cudaEventSynchronize(done[slot]);
+        const int did = std::min(batch, hs[slot]->iter - iter_seen);
+        iter_seen = hs[slot]->iter;
+        for (int k = 0; k < did; ++k) {
+          float ms = 0.f;
+          if (cudaEventElapsedTime(&ms, evs[2 * k], evs[2 * k + 1]) == cudaSuccess) {
+            c->timing.spmv_ms += ms;
+            c->timing.spmv_launches += 1;
+          }
+        }
+        in_flight = 1;
+        slot ^= 1;
+      }
+      if (in_flight == 0) {
+        in_flight = 1;
+        slot ^= 1;
+        continue;
+      }
+      const int prev = slot ^ 1;
+      cudaEventSynchronize(done[prev]);
+      const CgScalars* s = hs[prev];
+      if (!(s->stop || s->want_update)) {
+        slot ^= 1;
+        continue;
+      }
+      // act on the latest state
+      cudaEventSynchronize(done[slot]);
+      in_flight = 0;
+      const CgScalars cur = *hs[c->instrument ? prev : slot];
+      slot = 0;
+      if (cur.stop == 0 && !cur.want_update) continue;
+      status = true_residual(R, false);
+      if (status != UFC_STATUS_OK) break;
+      status = read_scalars(c);
+      if (status != UFC_STATUS_OK) break;
+      true_rr = c->h_scal->true_rr;
+      ++n_refine;
+      if (std::sqrt(true_rr) <= tol) {
+        converged = true;
+        finished = true;
+        break;
+      }
+      if (cur.stop == 2 || !std::isfinite(true_rr)) {
+        flag = std::isfinite(true_rr) ? 2 : 3;
+        finished = true;
+        break;
+      }
+      // progress of the FP64 residual across replacements; the best iterate is
+      // kept so that a stalled or diverging run can hand it on
+      if (true_rr < best_rr) {
+        if (keep_best) cudaMemcpyAsync(c->xb64, c->x64, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream);
+        if (true_rr < 0.25 * best_rr) stall = 0;
+        else ++stall;
+        best_rr = true_rr;
+      } else {
+        ++stall;
+      }
+      if (stall > kMaxStall || true_rr > kDiverge * best_rr) {
+        flag = 3;
+        finished = true;
+        if (keep_best) {  // hand on the best iterate and its residual
+          cudaMemcpyAsync(c->x64, c->xb64, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream);
+          true_rr = best_rr;
+        }
+        break;
+      }
+      int mode = cur.stop == 1 ? 1 : 0;
+      if (cur.stop == 3) {
+        // breakdown of the recurrence: restart CG from the FP64 residual
+        if (++restarts > kMaxRestarts) {
+          flag = 3;
+          finished = true;
+          if (keep_best) {
+            cudaMemcpyAsync(c->x64, c->xb64, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream);
+            true_rr = best_rr;
+          }
+          break;
+        }
+        mode = 2;
+      }
+      if (prec != UFC_PRECISION_FP64 && algo->refine_policy == UFC_REFINE_RESTART) mode = 2;
+      status = replace(R, V, mode);
+      if (status != UFC_STATUS_OK) break;
+    }
+    for (auto& e : evs) cudaEventDestroy(e);
+    cudaEventDestroy(done[0]);
+    cudaEventDestroy(done[1]);
+    if (status != UFC_STATUS_OK) return status;
+  }
+  UFC_TRY(read_scalars(c));
+  UFC_CUDA(c, cudaEventRecord(t1, c->stream));
+  UFC_CUDA(c, cudaEventSynchronize(t1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  c->timing.kernel_launches = c->launches;
+  st->niter = c->h_scal->iter;
+  st->n_refine = n_refine;
+  st->converged = converged ? 1 : 0;
+  st->convergence_flag = converged ? 0 : (flag ? flag : 2);
+  st->rnorm = std::sqrt(true_rr) / bnorm;
+  st->solve_time = ms;
+  UFC_TRY(check_dev_err(c, "ufc_pcg_solve"));
+  return converged ? UFC_STATUS_OK : UFC_STATUS_NOT_CONVERGED;
+}
+
+}  // namespace
+
+void release_graphs(Ctx* c) {
+  for (int k = 0; k < kGraphSlots; ++k) {
+    if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
+    c->cg_graph[k] = nullptr;
+    c->cg_graph_batch[k] = 0;
+    c->cg_graph_key[k] = nullptr;
+  }
+}
+
+int64_t spmv_bytes(const Ctx* c, int precision) {
+  // algorithmic bytes of one block-CSR SpMV: values + block column indices +
+  // block row pointers + x read once + y written once (slice padding excluded)
+  const int64_t sv = precision == UFC_PRECISION_FP64 ? 8 : 4;  // stored value
+  const int64_t sx = precision == UFC_PRECISION_FP32_REFINE ? 4 : 8;  // vector entry
+  return c->nnzb * (9 * sv + 4) + 4 * ((int64_t)c->N + 1) + 2 * c->n * sx;
+}
+
+int spmv(Ctx* c, int precision, const void* x, void* y) {
+  if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: pattern not built");
+  const int sg = (int)((c->nslices * kSlice + kSpmvBlock - 1) / kSpmvBlock);
+  const int64_t np = c->nslices * kSlice;
+  if (precision == UFC_PRECISION_FP64) {
+    if (!c->has_val64) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP64 values not assembled");
+    k_spmv<double, double, double, kPlain, false><<<sg, kSpmvBlock, 0, c->stream>>>(
+        c->N, np, c->slice_ptr, c->sell_col, c->val64, (const double*)x, (double*)y, nullptr, nullptr);
+  } else if (precision == UFC_PRECISION_FP32_REFINE) {
+    if (!c->has_val32) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP32 values not assembled");
+    if (c->val32_diff)
+      k_spmv<float, float, float, kPlain, true><<<sg, kSpmvBlock, 0, c->stream>>>(
+          c->N, np, c->slice_ptr, c->sell_col, c->val32, (const float*)x, (float*)y, nullptr, nullptr);
+    else
+      k_spmv<float, float, float, kPlain, false><<<sg, kSpmvBlock, 0, c->stream>>>(
+          c->N, np, c->slice_ptr, c->sell_col, c->val32, (const float*)x, (float*)y, nullptr, nullptr);
+  } else if (precision == UFC_PRECISION_FP32_MATRIX) {
+    if (!c->has_val32) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP32 values not assembled");
+    if (c->val32_diff)
+      k_spmv<float, double, double, kPlain, true><<<sg, kSpmvBlock, 0, c->stream>>>(
+          c->N, np, c->slice_ptr, c->sell_col, c->val32, (const double*)x, (double*)y, nullptr, nullptr);
+    else
+      k_spmv<float, double, double, kPlain, false><<<sg, kSpmvBlock, 0, c->stream>>>(
+          c->N, np, c->slice_ptr, c->sell_col, c->val32, (const double*)x, (double*)y, nullptr, nullptr);
+  } else {
+    return fail(c, UFC_STATUS_INVALID, "ufc_spmv: precision");
+  }
+  UFC_CUDA(c, cudaGetLastError());
+  return UFC_STATUS_OK;
+}
+
+int pcg_solve(Ctx* c, const double* b, double* x, const ufc_solver_algo* algo, ufc_solver_state* st) {
+  if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: pattern not built");
+  if (algo->method != UFC_SOLV_METHOD_CG) return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve: method must be CG");
+  if (algo->precond_type != UFC_SOLV_PREC_JACOBI && algo->precond_type != UFC_SOLV_PREC_NONE)
+    return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve: preconditioner must be Jacobi or none");
+  const int prec = algo->precision_mode;
+  if (prec == UFC_PRECISION_FP64 && !c->has_val64)
+    return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: FP64 values not assembled (UFC_BUILD_FP64)");
+  if (prec != UFC_PRECISION_FP64 && prec != UFC_PRECISION_FP32_REFINE && prec != UFC_PRECISION_FP32_MATRIX)
+    return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: precision_mode");
+  if (prec != UFC_PRECISION_FP64 && !c->has_val32)
+    return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: FP32 values not assembled (UFC_BUILD_FP32*)");
+  if (prec != UFC_PRECISION_FP64 && c->mat_model != UFC_MAT_ELASTIC_ISO)
+    return fail(c, UFC_STATUS_UNSUPPORTED,
+                "ufc_pcg_solve: FP32 matrices need the linear-elastic FP64 element operator for their residual");
+  if (prec == UFC_PRECISION_FP32_MATRIX && algo->precond_type == UFC_SOLV_PREC_JACOBI && !c->has_val64)
+    return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: FP32_MATRIX takes its Jacobi diagonal from the FP64 values");
+  UFC_TRY(ensure_vectors(c, prec));
+  UFC_CUDA(c, cudaMemcpyAsync(c->b64, b, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream));
+  if (algo->use_x0)
+    UFC_CUDA(c, cudaMemcpyAsync(c->x64, x, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream));
+  else
+    UFC_CUDA(c, cudaMemsetAsync(c->x64, 0, sizeof(double) * c->n, c->stream));
+  int s;
+  if (prec == UFC_PRECISION_FP64)
+    s = pcg_run<double, double, double>(c, algo, st);
+  else if (prec == UFC_PRECISION_FP32_MATRIX)
+    s = pcg_run<float, double, double>(c, algo, st);
+  else if (algo->accumulate == UFC_ACCUMULATE_FP64)
+    s = pcg_run<float, float, double>(c, algo, st);
+  else
+    s = pcg_run<float, float, float>(c, algo, st);
+  st->fp64_iters = 0;
+  if (s == UFC_STATUS_NOT_CONVERGED && prec != UFC_PRECISION_FP64 && st->convergence_flag == 3 && c->has_val64 &&
+      st->niter < algo->max_iter) {
+    // The FP32 matrix is too far from K for this problem (stall or divergence
+    // of the refined run): finish in FP64 from the best FP32 iterate.
+    ufc_solver_algo a64 = *algo;
+    a64.precision_mode = UFC_PRECISION_FP64;
+    a64.max_iter = algo->max_iter - st->niter;
+    ufc_solver_state s64{};
+    UFC_TRY(ensure_vectors(c, UFC_PRECISION_FP64));
+    s = pcg_run<double, double, double>(c, &a64, &s64);
+    if (s != UFC_STATUS_OK && s != UFC_STATUS_NOT_CONVERGED) return s;
+    st->fp64_iters = s64.niter;
+    st->niter += s64.niter;
+    st->n_refine += s64.n_refine;
+    st->converged = s64.converged;
+    st->convergence_flag = s64.convergence_flag;
+    st->rnorm = s64.rnorm;
+    st->solve_time += s64.solve_time;
+  }
+  if (s != UFC_STATUS_OK && s != UFC_STATUS_NOT_CONVERGED) return s;
+  UFC_CUDA(c, cudaMemcpyAsync(x, c->x64, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream));
+  if (s == UFC_STATUS_NOT_CONVERGED)
+    fail(c, UFC_STATUS_NOT_CONVERGED, "[NM_Solver_PCG]: did not converge");
+  return s;
+}
+
+}  // namespace ufc

@@ -1,0 +1,196 @@
+// Internal declarations of the B200 C3D8 hot path (not part of the C-ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ufc_gpu.h"
+
+namespace ufc {
+
+constexpr int kSlice = 32;       // rows per SELL slice = one warp
+constexpr int kMaxValence = 32;  // elements sharing one node (general hex meshes)
+constexpr int kMaxRowBlocks = 128;
+constexpr int kGraphSlots = 4;   // cached CG-batch graphs: one per solver type combination
+
+// Scalars of one CG run, kept on the device so iterations need no host sync.
+struct CgScalars {
+  double rz;        // r.z of the current iterate
+  double rz_old;    // r.z used by the last alpha
+  double pq;        // p.Ap
+  double alpha, beta;
+  double rr;        // ||r||^2 of the recursive residual
+  double rr_ref;    // ||r||^2 at the last FP64 residual replacement
+  double tol2;      // stop threshold on ||r||^2
+  double delta2;    // replacement trigger (FP32_REFINE)
+  double true_rr;   // ||b - K x||^2 from the last FP64 residual
+  double bb;        // ||b||^2
+  int32_t iter;
+  int32_t max_iter;
+  int32_t stop;     // 1 converged (recursive), 2 max-iter, 3 breakdown
+  int32_t want_update;
+  double nr_rr, nr_ff, nr_ee;  // Newton: ||R_free||^2, ||F_int||^2, ||F_ext||^2
+  uint32_t ticket[8];  // last-block election counters, one per reduction site
+};
+
+// Error word written by device kernels (never trap).
+enum DevErr : int32_t {
+  kDevOk = 0,
+  kDevBadJacobian = 1,
+  kDevNonFinite = 2,
+  kDevValence = 4,
+  kDevRowBlocks = 8,
+  kDevPattern = 16,
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;  // own non-blocking stream: all work runs here
+  cudaStream_t ext = nullptr;     // caller's stream, joined on entry and exit
+  bool has_ext = false;
+  cudaEvent_t ev_join = nullptr;
+  std::string err;
+  bool instrument = false;
+  ufc_timing_info timing{};
+  int64_t launches = 0;  // kernels enqueued by the library (counted at each launch site)
+
+  // mesh
+  int32_t N = 0, E = 0;
+  int64_t n = 0;
+  double* coords = nullptr;  // [N*3]
+  int32_t* conn = nullptr;   // [E*8], 0-based
+  std::vector<int32_t> h_conn;
+
+  // material
+  int32_t mat_model = 0, nprops = 0;
+  double* props = nullptr;  // [E*nprops]
+  bool has_material = false;
+
+  // colouring
+  int32_t ncol = 0;
+  std::vector<int32_t> col_off;      // ncol+1
+  int32_t* col_elems = nullptr;      // [E] elements grouped by colour, ascending inside a colour
+
+  // pattern: canonical block CSR + SELL-32 storage
+  bool has_pattern = false;
+  int64_t nnzb = 0;
+  int32_t max_row_blocks = 0;
+  int32_t* brow = nullptr;    // [N+1]
+  int32_t* bcol = nullptr;    // [nnzb]
+  int64_t nslices = 0, sell_blocks = 0;
+  int64_t* slice_ptr = nullptr;  // [nslices+1] block offsets
+  int32_t* sell_col = nullptr;   // [sell_blocks]
+  int32_t* slot = nullptr;       // [E*64] SELL position of block (a, b)
+  int32_t* dpos = nullptr;       // [N] SELL position of the diagonal block
+  double* val64 = nullptr;       // [sell_blocks*9]
+  float* val32 = nullptr;
+  bool has_val64 = false, has_val32 = false;
+  bool val32_diff = false;       // FP32 values in difference form (diagonal slot = block row sum)
+  double* dinv64 = nullptr;
+  float* dinv32 = nullptr;
+
+  // Dirichlet set
+  uint8_t* fixed = nullptr;  // [n]
+  int32_t nfix = 0;
+  int32_t* fix_dofs = nullptr;
+  double* fix_vals = nullptr;
+
+  // solver work
+  double *x64 = nullptr, *r64 = nullptr, *p64 = nullptr, *q64 = nullptr, *b64 = nullptr, *y64 = nullptr;
+  float *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+  double* xb64 = nullptr;  // best iterate of an FP32 run (handed to the FP64 continuation)
+  CgScalars* scal = nullptr;
+  double* partials = nullptr;   // [partials_cap] per-block partial sums of grid reductions
+  int64_t partials_cap = 0;
+  CgScalars* h_scal = nullptr;  // pinned mirror
+  int32_t* dev_err = nullptr;
+  int32_t* h_err = nullptr;     // pinned
+
+  // Newton work vectors
+  double *nr_fint = nullptr, *nr_R = nullptr, *nr_du = nullptr;
+
+  // displacement and J2 state
+  double* u = nullptr;      // [n] current
+  double* u_n = nullptr;    // [n] committed
+  double *sig_n = nullptr, *epeq_n = nullptr, *epl_n = nullptr;  // committed [G*6],[G],[G*6]
+  double *sig_t = nullptr, *epeq_t = nullptr, *epl_t = nullptr;  // trial
+  double* Dt = nullptr;     // [G*36] consistent tangent of the trial state
+  bool has_trial = false;
+
+  // cached CUDA graphs of CG batches
+  cudaGraphExec_t cg_graph[kGraphSlots] = {};
+  int cg_graph_batch[kGraphSlots] = {};
+  const void* cg_graph_key[kGraphSlots] = {};
+  std::vector<cudaEvent_t> ev_pool;
+};
+
+int grid_for(int64_t work, int block);
+int fail(Ctx* c, int status, const std::string& msg);
+int cuda_fail(Ctx* c, cudaError_t e, const char* where);
+int check_dev_err(Ctx* c, const char* where);
+
+// pattern.cu
+int build_pattern(Ctx* c);
+int export_csr(Ctx* c, const ufc_csr_export_arg* a);
+
+// c3d8.cu
+int assemble(Ctx* c, int build, double* elapsed_ms);
+int apply_fp64(Ctx* c, const double* x, double* y, bool masked);  // y = K x matrix-free, FP64
+int apply_fp64_eliminated(Ctx* c, const double* x, double* y);    // eliminated operator incl. identity rows
+int nr_norms(Ctx* c, const double* fext, const double* fint, double* R);  // R = fext - fint (free), norms
+int compute_fint(Ctx* c, const double* u, double* fint, bool update_state);
+int mat_update_batch(Ctx* c, const ufc_mat_update_arg* a, const double* props, const double* stress_n,
+                     const double* dstrain, const double* sdv_n, double* stress, double* sdv, double* ddsdde,
+                     int32_t* yielded);
+int stress_eval(Ctx* c, const double* u, double* sig, double* vm);
+int adjoint_sens(Ctx* c, int nrhs, const double* U, const double* L, double* g);
+int build_dinv(Ctx* c, int precision);
+
+// spmv.cu
+int spmv(Ctx* c, int precision, const void* x, void* y);
+int64_t spmv_bytes(const Ctx* c, int precision);
+
+// pcg.cu
+int pcg_solve(Ctx* c, const double* b, double* x, const ufc_solver_algo* algo, ufc_solver_state* st);
+int pcg_solve_block(Ctx* c, int nrhs, const double* B, double* X, const ufc_solver_algo* algo,
+                    ufc_solver_state* st);
+void release_graphs(Ctx* c);
+
+// device memory helper
+template <class T>
+int dalloc(Ctx* c, T** p, int64_t count) {
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  if (count <= 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (size_t)count);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return cuda_fail(c, e, "cudaMalloc");
+  }
+  return UFC_STATUS_OK;
+}
+
+template <class T>
+void dfree(T** p) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+}
+
+}  // namespace ufc
+
+#define UFC_TRY(expr)                      \
+  do {                                     \
+    int _s = (expr);                       \
+    if (_s != UFC_STATUS_OK) return _s;    \
+  } while (0)
+
+#define UFC_CUDA(c, expr)                                      \
+  do {                                                         \
+    cudaError_t _e = (expr);                                   \
+    if (_e != cudaSuccess) return ufc::cuda_fail((c), _e, #expr); \
+  } while (0)
