@@ -313,6 +313,24 @@ int ufc_get_state(ufc_ctx* ctx, double* eps_p_eq, double* stress, double* eps_p,
 int ufc_adjoint_sensitivity(ufc_ctx* ctx, int32_t nrhs, const double* U, const double* Lam, double* dJdE,
                             int32_t mem);
 
+/* ---- allocation-free SpMV (no counterpart in the reference) ----
+ * y = A x and *xy = x.y for a caller-owned FP64 CSR matrix (0-based row_ptr,
+ * col_ind, values, e.g. from ufc_csr_export with mem = UFC_MEM_DEVICE), all
+ * pointers in device memory, enqueued on cuda_stream (NULL: legacy stream).
+ * It is for callers that cannot allocate device memory -- a solver loop being
+ * captured into a CUDA graph, or a host code that owns all device memory in its
+ * own pool: it calls no cudaMalloc/cudaFree and needs no context.  The
+ * dot-product scratch is a static device array: at most UFC_NOALLOC_MAX_ROWS
+ * rows (larger calls return UFC_STATUS_INVALID); each GPU that loads the library
+ * keeps the array (about 512 KiB) until exit; the first call on a device looks
+ * up its address and should come before any stream capture; calls that overlap
+ * on the GPU share the array and race, so the caller serialises them.  The
+ * message of a failure is written to errbuf (may be NULL). */
+#define UFC_NOALLOC_MAX_ROWS 16777216
+int ufc_csr_spmv_dot_noalloc(int64_t n_rows, const int64_t* row_ptr, const int32_t* col_ind,
+                             const double* values, const double* x, double* y, double* xy, void* cuda_stream,
+                             char* errbuf, int32_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -141,6 +141,7 @@ _SIGS = {
     "ufc_set_displacement": [_p, _p, _i32],
     "ufc_get_state": [_p, _p, _p, _p, _i32],
     "ufc_adjoint_sensitivity": [_p, _i32, _p, _p, _p, _i32],
+    "ufc_csr_spmv_dot_noalloc": [_i64, _p, _p, _p, _p, _p, _p, _p, C.c_char_p, _i32],
 }
 
 _LIB = None
