@@ -172,11 +172,14 @@ class Model:
         self.fixed = np.zeros(self.n, dtype=np.uint8)
         self.fixed[p.fixed] = 1
 
-    def assemble(self, Dgp=None, props=None):
+    def assemble(self, Dgp=None, props=None, eliminate=True):
+        """Stiffness with the Dirichlet rows/columns eliminated, or the full
+        (singular) one when eliminate is False."""
         props = self.props if props is None else np.ascontiguousarray(props, dtype=np.float64)
         val = np.zeros(self.col.size)
         Dg = None if Dgp is None else np.ascontiguousarray(Dgp, dtype=np.float64)
-        st = lib().orc_assemble(self.N, self.E, self.coords, self.conn, props, props.shape[1], _ptr(Dg), self.fixed,
+        fixed = self.fixed if eliminate else np.zeros_like(self.fixed)
+        st = lib().orc_assemble(self.N, self.E, self.coords, self.conn, props, props.shape[1], _ptr(Dg), fixed,
                                 self.color, self.ncol, self.row_ptr, self.col, val)
         if st != 0:
             raise ValueError("non-positive Jacobian")
@@ -263,6 +266,9 @@ def nr_j2(model: Model, targets, tol=1e-8, max_iter=25, lin_rtol=1e-10):
     Convergence: ||R_free|| <= tol * max(||F_int||, 1e-30), F_int over every
     DOF (the reaction scale; the reference divides by ||F_ext||,
     RT_Step_NR_Core.f90:252-258, which is zero under displacement control).
+    The first iteration of an increment is the predictor
+    K_ff du_f = R_f - K_fc du_c (tangent at the start of the increment), after
+    which the prescribed DOFs take their new values.
     Returns the displacement history, the committed state and per-increment logs."""
     p = model.p
     G = model.E * 8
@@ -273,7 +279,9 @@ def nr_j2(model: Model, targets, tol=1e-8, max_iter=25, lin_rtol=1e-10):
     hist, logs = [], []
     for tgt in targets:
         u_n = u.copy()
-        u[p.fixed] = tgt
+        dc = np.zeros(model.n)
+        dc[p.fixed] = tgt - u[p.fixed]
+        lift = bool(np.any(dc != 0.0))
         log = []
         conv = False
         for it in range(max_iter):
@@ -283,12 +291,18 @@ def nr_j2(model: Model, targets, tol=1e-8, max_iter=25, lin_rtol=1e-10):
             rn = np.linalg.norm(R)
             fn = max(np.linalg.norm(fint), 1e-30)
             log.append(rn / fn)
-            if rn <= tol * fn:
+            if not lift and rn <= tol * fn:
                 conv = True
                 break
             K = model.assemble(Dgp=trial["D"])
+            if lift:
+                y = model.assemble(Dgp=trial["D"], eliminate=False).matvec(dc)
+                R[free] -= y[free]
             du, info = pcg(K, R, rtol=lin_rtol)
             u += du
+            if lift:
+                u[p.fixed] = tgt
+                lift = False
         if not conv:
             raise RuntimeError("NR did not converge")
         state = {"sig": trial["sig"], "epeq": trial["epeq"], "epl": trial["epl"]}

@@ -248,6 +248,50 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+// Matrix-free consistent-tangent operator, FP64, one thread per element of one
+// colour: y += sum_e B^T D_gp B x_e with the per-Gauss-point tangents of the
+// last return map (unmasked: all rows and columns).  Newton uses it to lift a
+// prescribed displacement increment into the right-hand side.
+__global__ void __launch_bounds__(128)
+    k_apply_tangent(const int32_t* __restrict__ elems, int32_t ne, const double* __restrict__ coords,
+                    const int32_t* __restrict__ conn, const double* __restrict__ Dt, const double* __restrict__ x,
+                    double* __restrict__ y) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ne) return;
+  const int64_t e = elems[idx];
+  int64_t nd[8];
+  double X[24], xe[24], fe[24];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    nd[a] = conn[e * 8 + a];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      X[a * 3 + i] = coords[nd[a] * 3 + i];
+      xe[a * 3 + i] = x[3 * nd[a] + i];
+      fe[a * 3 + i] = 0.0;
+    }
+  }
+#pragma unroll 1
+  for (int ip = 0; ip < 8; ++ip) {
+    double inv[9], eps[6], s[6];
+    const double det = jacobian_inv<double>(X, ip, inv);
+    strain_at<double>(inv, ip, xe, eps);
+    const double* D = Dt + (e * 8 + ip) * 36;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      double t = 0.0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) t += D[i * 6 + j] * eps[j];
+      s[i] = t;
+    }
+    add_bt_sigma<double>(inv, ip, det, s, fe);
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) y[3 * nd[a] + i] += fe[a * 3 + i];
+}
+
 // J2 return map at every Gauss point: strain increment from du = u - u_n,
 // committed state (sig_n, epeq_n, epl_n) -> trial state and consistent tangent.
 __global__ void __launch_bounds__(128)
@@ -639,6 +683,19 @@ int compute_fint(Ctx* c, const double* u, double* fint, bool update_state) {
     if (ne == 0) continue;
     k_fint_from_stress<<<grid_for(ne, 128), 128, 0, c->stream>>>(c->col_elems + c->col_off[col], ne, c->coords,
                                                                  c->conn, c->sig_t, fint);
+    UFC_CUDA(c, cudaGetLastError());
+  }
+  return UFC_STATUS_OK;
+}
+
+int apply_tangent(Ctx* c, const double* x, double* y) {
+  if (!c->has_trial) return fail(c, UFC_STATUS_INVALID, "tangent operator needs a return map first");
+  UFC_CUDA(c, cudaMemsetAsync(y, 0, sizeof(double) * c->n, c->stream));
+  for (int col = 0; col < c->ncol; ++col) {
+    const int32_t ne = c->col_off[col + 1] - c->col_off[col];
+    if (ne == 0) continue;
+    k_apply_tangent<<<grid_for(ne, 128), 128, 0, c->stream>>>(c->col_elems + c->col_off[col], ne, c->coords, c->conn,
+                                                              c->Dt, x, y);
     UFC_CUDA(c, cudaGetLastError());
   }
   return UFC_STATUS_OK;

@@ -135,7 +135,7 @@ void free_all(Ctx* c) {
   dfree(&c->fixed); dfree(&c->fix_dofs); dfree(&c->fix_vals);
   dfree(&c->x64); dfree(&c->r64); dfree(&c->p64); dfree(&c->q64); dfree(&c->b64); dfree(&c->y64);
   dfree(&c->r32); dfree(&c->p32); dfree(&c->q32); dfree(&c->xb64);
-  dfree(&c->nr_fint); dfree(&c->nr_R); dfree(&c->nr_du);
+  dfree(&c->nr_fint); dfree(&c->nr_R); dfree(&c->nr_du); dfree(&c->nr_dc);
   dfree(&c->u); dfree(&c->u_n);
   dfree(&c->sig_n); dfree(&c->epeq_n); dfree(&c->epl_n); dfree(&c->sig_t); dfree(&c->epeq_t); dfree(&c->epl_t);
   dfree(&c->Dt);
@@ -163,6 +163,24 @@ __global__ void k_set_vals(int32_t nfix, const int32_t* __restrict__ dofs, const
                            double* __restrict__ u) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nfix) u[dofs[i]] = vals ? vals[i] : 0.0;
+}
+
+// dc[dof] = target - u[dof] on the Dirichlet DOFs (dc is zero elsewhere);
+// flags *changed when any prescribed value moves.
+__global__ void k_prescribed_delta(int32_t nfix, const int32_t* __restrict__ dofs, const double* __restrict__ vals,
+                                   const double* __restrict__ u, double* __restrict__ dc, int32_t* __restrict__ changed) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nfix) return;
+  const double d = vals[i] - u[dofs[i]];
+  dc[dofs[i]] = d;
+  if (d != 0.0) atomicOr(changed, 1);
+}
+
+// R -= y on the free DOFs (R is zero on the fixed ones).
+__global__ void k_sub_free(int64_t n, const uint8_t* __restrict__ fixed, const double* __restrict__ y,
+                           double* __restrict__ R) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (!fixed[i]) R[i] -= y[i];
 }
 
 __global__ void k_axpy(int64_t n, double a, const double* __restrict__ x, double* __restrict__ y) {
@@ -560,16 +578,25 @@ int ufc_nr_increment(ufc_ctx* c, ufc_nr_arg* a) {
   if (!c->nr_fint) UFC_TRY(dalloc(c, &c->nr_fint, c->n));
   if (!c->nr_R) UFC_TRY(dalloc(c, &c->nr_R, c->n));
   if (!c->nr_du) UFC_TRY(dalloc(c, &c->nr_du, c->n));
-  // prescribed values at the end of the increment
-  if (c->nfix > 0) {
-    if (up.dev)
-      UFC_CUDA(c, cudaMemcpyAsync(c->fix_vals, up.dev, sizeof(double) * c->nfix, cudaMemcpyDeviceToDevice, c->stream));
-    k_set_vals<<<grid_for(c->nfix, 256), 256, 0, c->stream>>>(c->nfix, c->fix_dofs, c->fix_vals, c->u);
+  if (!c->nr_dc) UFC_TRY(dalloc(c, &c->nr_dc, c->n));
+  // prescribed values at the end of the increment, and their change du_c
+  bool lift = false;
+  if (c->nfix > 0 && up.dev) {
+    UFC_CUDA(c, cudaMemcpyAsync(c->fix_vals, up.dev, sizeof(double) * c->nfix, cudaMemcpyDeviceToDevice, c->stream));
+    UFC_CUDA(c, cudaMemsetAsync(c->nr_dc, 0, sizeof(double) * c->n, c->stream));
+    k_prescribed_delta<<<grid_for(c->nfix, 256), 256, 0, c->stream>>>(c->nfix, c->fix_dofs, c->fix_vals, c->u,
+                                                                      c->nr_dc, c->dev_err);
     UFC_CUDA(c, cudaGetLastError());
+    UFC_CUDA(c, cudaMemcpyAsync(c->h_err, c->dev_err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    UFC_TRY(sync(c));
+    lift = *c->h_err != 0;  // some prescribed value changed
+    UFC_CUDA(c, cudaMemsetAsync(c->dev_err, 0, sizeof(int32_t), c->stream));
   }
   ufc_solver_algo lin = a->lin;
   lin.use_x0 = 0;
-  const int build = lin.precision_mode == UFC_PRECISION_FP32_REFINE ? (UFC_BUILD_FP32 | UFC_BUILD_FP64) : UFC_BUILD_FP64;
+  const int build = UFC_BUILD_FP64;  // the tangent is not the linear-elastic operator: FP64 CG
+  lin.precision_mode = UFC_PRECISION_FP64;
+  const int vg = std::min(grid_for(c->n, 256), 148 * 8);
   for (int it = 0; it < a->max_iterations; ++it) {
     UFC_TRY(compute_fint(c, c->u, c->nr_fint, true));
     UFC_TRY(nr_norms(c, fe.dev, c->nr_fint, c->nr_R));
@@ -581,19 +608,31 @@ int ufc_nr_increment(ufc_ctx* c, ufc_nr_arg* a) {
     a->res_hist[it] = rn / ref;
     a->residual_norm = rn / ref;
     if (!std::isfinite(rn)) return fail(c, UFC_STATUS_ERROR, "ufc_nr_increment: non-finite residual");
-    if (rn <= a->tolerance_force * ref) {
+    if (!lift && rn <= a->tolerance_force * ref) {
       a->converged = 1;
       a->iterations = it;
       break;
     }
     ufc_elem_ke_arg ka{};
     UFC_TRY(assemble(c, build, &ka.elapsed_ms));
+    if (lift) {
+      // predictor: K_ff du_f = R_f - K_fc du_c with the tangent of the start of the
+      // increment, then u_c takes its prescribed values
+      UFC_TRY(apply_tangent(c, c->nr_dc, c->nr_du));
+      k_sub_free<<<vg, 256, 0, c->stream>>>(c->n, c->fixed, c->nr_du, c->nr_R);
+      UFC_CUDA(c, cudaGetLastError());
+    }
     ufc_solver_state ls{};
     const int s = pcg_solve(c, c->nr_R, c->nr_du, &lin, &ls);
     a->lin_iters_total += ls.niter;
     if (s != UFC_STATUS_OK) return s;
-    k_axpy<<<std::min(grid_for(c->n, 256), 148 * 8), 256, 0, c->stream>>>(c->n, 1.0, c->nr_du, c->u);
+    k_axpy<<<vg, 256, 0, c->stream>>>(c->n, 1.0, c->nr_du, c->u);
     UFC_CUDA(c, cudaGetLastError());
+    if (lift) {
+      k_set_vals<<<grid_for(c->nfix, 256), 256, 0, c->stream>>>(c->nfix, c->fix_dofs, c->fix_vals, c->u);
+      UFC_CUDA(c, cudaGetLastError());
+      lift = false;
+    }
     a->iterations = it + 1;
   }
   a->status = a->converged ? UFC_STATUS_OK : UFC_STATUS_NOT_CONVERGED;

@@ -110,7 +110,7 @@ struct Ctx {
   int32_t* h_err = nullptr;     // pinned
 
   // Newton work vectors
-  double *nr_fint = nullptr, *nr_R = nullptr, *nr_du = nullptr;
+  double *nr_fint = nullptr, *nr_R = nullptr, *nr_du = nullptr, *nr_dc = nullptr;
 
   // displacement and J2 state
   double* u = nullptr;      // [n] current
@@ -142,6 +142,7 @@ int apply_fp64(Ctx* c, const double* x, double* y, bool masked);  // y = K x mat
 int apply_fp64_eliminated(Ctx* c, const double* x, double* y);    // eliminated operator incl. identity rows
 int nr_norms(Ctx* c, const double* fext, const double* fint, double* R);  // R = fext - fint (free), norms
 int compute_fint(Ctx* c, const double* u, double* fint, bool update_state);
+int apply_tangent(Ctx* c, const double* x, double* y);  // y = K_tangent x, matrix-free, all DOFs
 int mat_update_batch(Ctx* c, const ufc_mat_update_arg* a, const double* props, const double* stress_n,
                      const double* dstrain, const double* sdv_n, double* stress, double* sdv, double* ddsdde,
                      int32_t* yielded);
