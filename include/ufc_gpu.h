@@ -84,6 +84,11 @@ extern "C" {
 #define UFC_BUILD_FP32 2
 #define UFC_BUILD_FP32_ROUNDED 4
 #define UFC_BUILD_FP32_DIFF 8
+/* Also pack symmetric SpMV copies (upper-triangle blocks only; each row reads
+ * its lower blocks transposed from the rows that store them): FP64, and FP32
+ * rounded from FP64 when an FP32 build is requested.  The solver and ufc_spmv
+ * use them when present.  Implies UFC_BUILD_FP64. */
+#define UFC_BUILD_SYMMETRIC 16
 
 /* FP32_REFINE policy at each FP64 residual replacement. */
 #define UFC_REFINE_KEEP_DIRECTION 0 /* keep the search direction (reliable update) */
@@ -295,6 +300,10 @@ int ufc_pcg_solve(ufc_ctx* ctx, const double* b, double* x, int32_t mem, const u
 int ufc_pcg_solve_block(ufc_ctx* ctx, int32_t nrhs, const double* B, double* X, int32_t mem,
                         const ufc_solver_algo* algo, ufc_solver_state* states);
 int ufc_last_timing(const ufc_ctx* ctx, ufc_timing_info* info);
+/* NM_Solver_State%residual_history (NM_Solv_Def.f90:114) of the last solve:
+ * ||r_k||_2 of the CG recurrence after each iteration k (host array, at most
+ * max_len entries, the count in *len; the first 2^20 iterations are kept). */
+int ufc_last_residual_history(ufc_ctx* ctx, double* out, int32_t max_len, int32_t* len);
 
 /* ---- nonlinear driver and material state (RT_Step_Exec.f90:415-600) ---- */
 int ufc_nr_increment(ufc_ctx* ctx, ufc_nr_arg* arg);

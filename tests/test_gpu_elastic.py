@@ -122,6 +122,32 @@ def test_cantilever_40x8x8_solve(pkg, orc, prec):
         assert abs(st.niter - info10["iters"]) <= 3, (st.niter, info10["iters"])
 
 
+@pytest.mark.parametrize("shape", [(8, 4, 4), (33, 5, 3)])
+def test_symmetric_storage_matches_full(pkg, orc, shape):
+    p = pkg.mesh.lognormal_cantilever(*shape, seed=6)
+    full = _model(pkg, p, pkg.BUILD_FP64 | pkg.BUILD_FP32_ROUNDED)
+    sym = _model(pkg, p, pkg.BUILD_FP64 | pkg.BUILD_FP32_ROUNDED | pkg.BUILD_SYMMETRIC)
+    K = orc.Model(p).assemble()
+    x = np.random.default_rng(1).standard_normal(p.n_dof)
+    y_o = K.matvec(x)
+    scale = np.abs(y_o).max()
+    assert np.abs(sym.spmv(x) - y_o).max() <= 1e-13 * scale
+    x32 = x.astype(np.float32)
+    y32_full = full.spmv(x32, precision=pkg.PRECISION_FP32_REFINE)
+    y32_sym = sym.spmv(x32, precision=pkg.PRECISION_FP32_REFINE)
+    assert np.abs(y32_sym - y32_full).max() <= 1e-5 * scale
+    assert np.abs(y32_sym - y_o).max() <= 1e-5 * scale
+    b = pkg.lifted_rhs(sym, p.f)
+    u_ref, _ = orc.Model(p).solve_linear(rtol=1e-13)
+    for prec in (pkg.PRECISION_FP64, pkg.PRECISION_FP32_REFINE):
+        u, st = sym.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=prec))
+        assert st.converged and st.rnorm <= 1e-10
+        assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-8
+    # the canonical export is unchanged by the symmetric copies
+    _, _, v, _ = sym.csr_export()
+    assert np.abs(v - K.val).max() <= 1e-12 * np.abs(K.val).max()
+
+
 def test_cantilever_beam_theory(pkg):
     # E2E_C2_01 checks tip deflection against beam theory within 5 % (with
     # incompatible modes); full-integration C3D8 on 40x8x8 is within 5 % of

@@ -24,6 +24,7 @@ BUILD_FP64 = _abi.BUILD_FP64
 BUILD_FP32 = _abi.BUILD_FP32
 BUILD_FP32_ROUNDED = _abi.BUILD_FP32_ROUNDED
 BUILD_FP32_DIFF = _abi.BUILD_FP32_DIFF
+BUILD_SYMMETRIC = _abi.BUILD_SYMMETRIC
 REFINE_KEEP_DIRECTION = _abi.REFINE_KEEP_DIRECTION
 REFINE_RESTART = _abi.REFINE_RESTART
 MAT_ELASTIC_ISO = _abi.MAT_ELASTIC_ISO

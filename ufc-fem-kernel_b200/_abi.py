@@ -45,6 +45,7 @@ BUILD_FP64 = 1
 BUILD_FP32 = 2
 BUILD_FP32_ROUNDED = 4
 BUILD_FP32_DIFF = 8
+BUILD_SYMMETRIC = 16
 REFINE_KEEP_DIRECTION = 0
 REFINE_RESTART = 1
 
@@ -134,6 +135,7 @@ _SIGS = {
     "ufc_pcg_solve": [_p, _p, _p, _i32, C.POINTER(SolverAlgo), C.POINTER(SolverState)],
     "ufc_pcg_solve_block": [_p, _i32, _p, _p, _i32, C.POINTER(SolverAlgo), C.POINTER(SolverState)],
     "ufc_last_timing": [_p, C.POINTER(TimingInfo)],
+    "ufc_last_residual_history": [_p, _p, _i32, C.POINTER(_i32)],
     "ufc_nr_increment": [_p, C.POINTER(NrArg)],
     "ufc_state_commit": [_p],
     "ufc_state_rollback": [_p],

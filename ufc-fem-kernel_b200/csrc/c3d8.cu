@@ -515,6 +515,7 @@ int assemble(Ctx* c, int build, double* elapsed_ms) {
     return fail(c, UFC_STATUS_INVALID,
                 "ufc_elem_compute_ke: J2 tangent needs ufc_elem_compute_fint(update_state=1) first");
   UFC_TRY(ensure_pairs(c));
+  release_graphs(c);  // captured CG batches hold pointers to the values they read
   cudaEvent_t e0, e1;
   UFC_CUDA(c, cudaEventCreate(&e0));
   UFC_CUDA(c, cudaEventCreate(&e1));
@@ -523,7 +524,11 @@ int assemble(Ctx* c, int build, double* elapsed_ms) {
   const int64_t nv = c->sell_blocks * 9;
   const bool diff = (build & UFC_BUILD_FP32_DIFF) != 0;
   const bool rounded = diff || (build & UFC_BUILD_FP32_ROUNDED) != 0;
+  const bool sym = (build & UFC_BUILD_SYMMETRIC) != 0;
+  const bool sym32 = sym && (build & (UFC_BUILD_FP32 | UFC_BUILD_FP32_ROUNDED | UFC_BUILD_FP32_DIFF)) != 0;
   if (rounded) build = (build | UFC_BUILD_FP64) & ~UFC_BUILD_FP32;
+  if (sym) build |= UFC_BUILD_FP64;
+  c->has_sval64 = c->has_sval32 = false;  // values change: symmetric copies are stale
   if (build & UFC_BUILD_FP32) c->val32_diff = false;
   for (int prec = 0; prec < 2; ++prec) {
     const bool want = prec == 0 ? (build & UFC_BUILD_FP64) : (build & UFC_BUILD_FP32);
@@ -589,6 +594,7 @@ int assemble(Ctx* c, int build, double* elapsed_ms) {
     c->val32_diff = diff;
     release_graphs(c);  // the SpMV form changed
   }
+  if (sym) UFC_TRY(pack_symmetric(c, true, sym32));
   UFC_CUDA(c, cudaEventRecord(e1, c->stream));
   UFC_CUDA(c, cudaEventSynchronize(e1));
   float ms = 0.f;

@@ -132,9 +132,13 @@ void free_all(Ctx* c) {
   dfree(&c->coords); dfree(&c->conn); dfree(&c->props); dfree(&c->col_elems);
   dfree(&c->brow); dfree(&c->bcol); dfree(&c->slice_ptr); dfree(&c->sell_col); dfree(&c->slot); dfree(&c->dpos);
   dfree(&c->val64); dfree(&c->val32); dfree(&c->dinv64); dfree(&c->dinv32);
+  dfree(&c->uptr); dfree(&c->ucol); dfree(&c->lptr); dfree(&c->lpos); dfree(&c->lcol); dfree(&c->s_lcnt);
+  dfree(&c->sval64); dfree(&c->sval32);
+  c->has_sym_pattern = c->has_sval64 = c->has_sval32 = false;
   dfree(&c->fixed); dfree(&c->fix_dofs); dfree(&c->fix_vals);
   dfree(&c->x64); dfree(&c->r64); dfree(&c->p64); dfree(&c->q64); dfree(&c->b64); dfree(&c->y64);
-  dfree(&c->r32); dfree(&c->p32); dfree(&c->q32); dfree(&c->xb64);
+  dfree(&c->r32); dfree(&c->p32); dfree(&c->q32); dfree(&c->xb64); dfree(&c->hist);
+  c->hist_cap = c->hist_len = 0;
   dfree(&c->nr_fint); dfree(&c->nr_R); dfree(&c->nr_du); dfree(&c->nr_dc);
   dfree(&c->u); dfree(&c->u_n);
   dfree(&c->sig_n); dfree(&c->epeq_n); dfree(&c->epl_n); dfree(&c->sig_t); dfree(&c->epeq_t); dfree(&c->epl_t);
@@ -350,7 +354,7 @@ int ufc_material_set(ufc_ctx* c, const ufc_material_desc* m) {
   UFC_CUDA(c, cudaMemcpyAsync(c->props, full.data(), sizeof(double) * full.size(), cudaMemcpyHostToDevice, c->stream));
   UFC_TRY(alloc_state(c));
   c->has_material = true;
-  c->has_val64 = c->has_val32 = false;  // values depend on the material
+  c->has_val64 = c->has_val32 = c->has_sval64 = c->has_sval32 = false;  // values depend on the material
   return sync(c);
 }
 
@@ -386,7 +390,7 @@ int ufc_bc_set(ufc_ctx* c, const ufc_bc_desc* bc) {
     UFC_CUDA(c, cudaMemcpyAsync(c->fix_vals, v.data(), sizeof(double) * c->nfix, cudaMemcpyHostToDevice, c->stream));
   }
   UFC_CUDA(c, cudaMemcpyAsync(c->fixed, mask.data(), c->n, cudaMemcpyHostToDevice, c->stream));
-  c->has_val64 = c->has_val32 = false;  // elimination is part of the values
+  c->has_val64 = c->has_val32 = c->has_sval64 = c->has_sval32 = false;  // elimination is part of the values
   return sync(c);
 }
 
@@ -415,7 +419,8 @@ int ufc_csr_export(ufc_ctx* c, const ufc_csr_export_arg* a) {
 
 int ufc_elem_compute_ke(ufc_ctx* c, ufc_elem_ke_arg* a) {
   CTX_CHECK(c);
-  if (!a || (a->build & (UFC_BUILD_FP64 | UFC_BUILD_FP32 | UFC_BUILD_FP32_ROUNDED | UFC_BUILD_FP32_DIFF)) == 0)
+  if (!a || (a->build & (UFC_BUILD_FP64 | UFC_BUILD_FP32 | UFC_BUILD_FP32_ROUNDED | UFC_BUILD_FP32_DIFF |
+                         UFC_BUILD_SYMMETRIC)) == 0)
     return fail(c, UFC_STATUS_INVALID, "ufc_elem_compute_ke: build must select FP64 and/or FP32");
   Scope sc(c);
   a->status = assemble(c, a->build, &a->elapsed_ms);
@@ -558,6 +563,19 @@ int ufc_pcg_solve_block(ufc_ctx* c, int32_t nrhs, const double* B, double* X, in
 int ufc_last_timing(const ufc_ctx* c, ufc_timing_info* info) {
   if (!c || !info) return UFC_STATUS_INVALID;
   *info = c->timing;
+  return UFC_STATUS_OK;
+}
+
+int ufc_last_residual_history(ufc_ctx* c, double* out, int32_t max_len, int32_t* len) {
+  CTX_CHECK(c);
+  if (!out || !len || max_len < 0) return fail(c, UFC_STATUS_INVALID, "ufc_last_residual_history: NULL argument");
+  Scope sc(c);
+  const int32_t k = std::min(max_len, c->hist_len);
+  *len = k;
+  if (k == 0) return UFC_STATUS_OK;
+  UFC_CUDA(c, cudaMemcpyAsync(out, c->hist, sizeof(double) * k, cudaMemcpyDeviceToHost, c->stream));
+  UFC_TRY(sync(c));
+  for (int32_t i = 0; i < k; ++i) out[i] = std::sqrt(out[i]);
   return UFC_STATUS_OK;
 }
 

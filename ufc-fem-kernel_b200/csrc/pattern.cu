@@ -171,6 +171,99 @@ __global__ void k_slots(int32_t E, const int32_t* __restrict__ conn, const int32
   }
 }
 
+// Position of column v in canonical block row r (binary search), or -1.
+__device__ __forceinline__ int find_in_row(const int32_t* __restrict__ brow, const int32_t* __restrict__ bcol,
+                                           int64_t r, int32_t v) {
+  int lo = brow[r], hi = brow[r + 1] - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int32_t x = bcol[mid];
+    if (x < v) lo = mid + 1;
+    else if (x > v) hi = mid - 1;
+    else return mid - brow[r];
+  }
+  return -1;
+}
+
+// Lower (j < i) and upper (j >= i) block counts of every row.
+__global__ void k_sym_counts(int32_t N, const int32_t* __restrict__ brow, const int32_t* __restrict__ bcol,
+                             int32_t* __restrict__ lcnt, int32_t* __restrict__ ucnt) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int d = find_in_row(brow, bcol, i, (int32_t)i);  // the diagonal is always present
+  lcnt[i] = d;
+  ucnt[i] = brow[i + 1] - brow[i] - d;
+}
+
+__global__ void k_slice_len_counts(int32_t N, int64_t nslices, const int32_t* __restrict__ cnt,
+                                   int64_t* __restrict__ len) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslices) return;
+  int32_t m = 0;
+  for (int t = 0; t < kSlice; ++t) {
+    const int64_t r = s * kSlice + t;
+    if (r < N) m = max(m, cnt[r]);
+  }
+  len[s] = (int64_t)m * kSlice;
+}
+
+// Symmetric storage index arrays, one thread per (padded) row: upper columns
+// (padding points at the row itself, zero values) and, for every lower block
+// (j, i), its position in row j's upper storage (padding points at the zero
+// slice appended after the last stored block).
+__global__ void k_sym_fill(int32_t N, int64_t nslices, const int32_t* __restrict__ brow,
+                           const int32_t* __restrict__ bcol, const int32_t* __restrict__ lcnt,
+                           const int64_t* __restrict__ uptr, const int64_t* __restrict__ lptr, int64_t zero_pos,
+                           int32_t* __restrict__ ucol, int32_t* __restrict__ lpos, int32_t* __restrict__ lcol,
+                           int32_t* __restrict__ err) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nslices * kSlice) return;
+  const int64_t s = r / kSlice, t = r % kSlice;
+  const int64_t ub = uptr[s], ul = (uptr[s + 1] - ub) / kSlice;
+  const int64_t lb = lptr[s], ll = (lptr[s + 1] - lb) / kSlice;
+  const bool real = r < N;
+  const int32_t b = real ? brow[r] : 0;
+  const int32_t nl = real ? lcnt[r] : 0;
+  const int32_t nu = real ? brow[r + 1] - b - nl : 0;
+  const int32_t self = real ? (int32_t)r : 0;
+  for (int64_t j = 0; j < ul; ++j) ucol[ub + j * kSlice + t] = j < nu ? bcol[b + nl + j] : self;
+  // lower entries in descending column order: the k-th lower entry of row r is
+  // then paired with (about) the k-th upper entry of the row that stores it, so
+  // the SpMV touches both within one loop step and the second read hits L2
+  for (int64_t j = 0; j < ll; ++j) {
+    int32_t pos = (int32_t)zero_pos, cj = 0;
+    if (j < nl) {
+      cj = bcol[b + nl - 1 - j];  // cj < r: block (cj, r) lives in row cj's upper part
+      const int k = find_in_row(brow, bcol, cj, (int32_t)r);
+      if (k < 0) {
+        atomicOr(err, (int)kDevPattern);
+      } else {
+        const int64_t sj = cj / kSlice, tj = cj % kSlice;
+        pos = (int32_t)(uptr[sj] + (int64_t)(k - lcnt[cj]) * kSlice + tj);
+      }
+    }
+    lpos[lb + j * kSlice + t] = pos;
+    lcol[lb + j * kSlice + t] = cj;
+  }
+}
+
+// Copy the upper blocks of the full SELL values into the symmetric storage.
+template <typename TO>
+__global__ void k_sym_pack(int32_t N, const int64_t* __restrict__ sptr, const int64_t* __restrict__ uptr,
+                           const int32_t* __restrict__ brow, const int32_t* __restrict__ lcnt,
+                           const double* __restrict__ v64, TO* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int64_t s = i / kSlice, t = i % kSlice;
+  const int32_t nl = lcnt[i], nu = brow[i + 1] - brow[i] - nl;
+  for (int32_t j = 0; j < nu; ++j) {
+    const int64_t src = sptr[s] + (int64_t)(nl + j) * kSlice + t;
+    const int64_t dst = uptr[s] + (int64_t)j * kSlice + t;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) out[vpos(dst, c)] = (TO)v64[vpos(src, c)];
+  }
+}
+
 // Scalar CSR export from the block pattern, one thread per (block row, entry).
 template <typename TV>
 __global__ void k_export(int32_t N, const int32_t* __restrict__ brow, const int32_t* __restrict__ bcol,
@@ -251,6 +344,9 @@ int scan_exclusive(Ctx* c, const T* in, T* out, int64_t n) {
 int build_pattern(Ctx* c) {
   if (c->E <= 0 || c->N <= 0) return fail(c, UFC_STATUS_INVALID, "ufc_pattern_build: mesh not set");
   release_graphs(c);
+  dfree(&c->uptr); dfree(&c->ucol); dfree(&c->lptr); dfree(&c->lpos); dfree(&c->lcol); dfree(&c->s_lcnt);
+  dfree(&c->sval64); dfree(&c->sval32);
+  c->has_sym_pattern = c->has_sval64 = c->has_sval32 = false;
   const int32_t N = c->N, E = c->E;
 
   // 1. colouring (host) and colour-grouped element lists
@@ -407,6 +503,72 @@ int export_csr(Ctx* c, const ufc_csr_export_arg* a) {
     UFC_CUDA(c, cudaStreamSynchronize(c->stream));
     dfree(&d_rp); dfree(&d_col); dfree(&d_v64); dfree(&d_v32);
   }
+  return UFC_STATUS_OK;
+}
+
+int build_sym_pattern(Ctx* c) {
+  if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "symmetric storage: pattern not built");
+  if (c->has_sym_pattern) return UFC_STATUS_OK;
+  const int32_t N = c->N;
+  int32_t* ucnt = nullptr;
+  int64_t* len = nullptr;
+  UFC_TRY(dalloc(c, &c->s_lcnt, N));
+  UFC_TRY(dalloc(c, &ucnt, N));
+  UFC_TRY(dalloc(c, &len, c->nslices + 1));
+  k_sym_counts<<<grid_for(N, 128), 128, 0, c->stream>>>(N, c->brow, c->bcol, c->s_lcnt, ucnt);
+  UFC_CUDA(c, cudaMemsetAsync(len, 0, sizeof(int64_t) * (c->nslices + 1), c->stream));
+  k_slice_len_counts<<<grid_for(c->nslices, 256), 256, 0, c->stream>>>(N, c->nslices, ucnt, len);
+  UFC_TRY(dalloc(c, &c->uptr, c->nslices + 1));
+  UFC_TRY(scan_exclusive(c, len, c->uptr, c->nslices + 1));
+  UFC_CUDA(c, cudaMemsetAsync(len, 0, sizeof(int64_t) * (c->nslices + 1), c->stream));
+  k_slice_len_counts<<<grid_for(c->nslices, 256), 256, 0, c->stream>>>(N, c->nslices, c->s_lcnt, len);
+  UFC_TRY(dalloc(c, &c->lptr, c->nslices + 1));
+  UFC_TRY(scan_exclusive(c, len, c->lptr, c->nslices + 1));
+  UFC_CUDA(c, cudaGetLastError());
+  UFC_CUDA(c, cudaMemcpyAsync(&c->s_ublocks, c->uptr + c->nslices, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                              c->stream));
+  UFC_CUDA(c, cudaMemcpyAsync(&c->s_lblocks, c->lptr + c->nslices, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                              c->stream));
+  UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  dfree(&len);
+  dfree(&ucnt);
+  if (c->s_ublocks + kSlice >= ((int64_t)1 << 31))
+    return fail(c, UFC_STATUS_UNSUPPORTED, "symmetric storage: more than 2^31 stored blocks");
+  UFC_TRY(dalloc(c, &c->ucol, c->s_ublocks));
+  UFC_TRY(dalloc(c, &c->lpos, std::max<int64_t>(c->s_lblocks, 1)));
+  UFC_TRY(dalloc(c, &c->lcol, std::max<int64_t>(c->s_lblocks, 1)));
+  UFC_CUDA(c, cudaMemsetAsync(c->dev_err, 0, sizeof(int32_t), c->stream));
+  k_sym_fill<<<grid_for(c->nslices * kSlice, 128), 128, 0, c->stream>>>(
+      N, c->nslices, c->brow, c->bcol, c->s_lcnt, c->uptr, c->lptr, c->s_ublocks, c->ucol, c->lpos, c->lcol,
+      c->dev_err);
+  UFC_CUDA(c, cudaGetLastError());
+  UFC_TRY(check_dev_err(c, "symmetric storage"));
+  c->has_sym_pattern = true;
+  return UFC_STATUS_OK;
+}
+
+int pack_symmetric(Ctx* c, bool fp64, bool fp32) {
+  if (!c->has_val64) return fail(c, UFC_STATUS_INVALID, "symmetric storage: FP64 values not assembled");
+  UFC_TRY(build_sym_pattern(c));
+  // stored blocks plus one zero slice that padded lower references point at
+  const int64_t nv = (c->s_ublocks + kSlice) * 9;
+  if (fp64) {
+    if (!c->sval64) UFC_TRY(dalloc(c, &c->sval64, nv));
+    UFC_CUDA(c, cudaMemsetAsync(c->sval64, 0, sizeof(double) * nv, c->stream));
+    k_sym_pack<double><<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->N, c->slice_ptr, c->uptr, c->brow, c->s_lcnt,
+                                                                   c->val64, c->sval64);
+    UFC_CUDA(c, cudaGetLastError());
+    c->has_sval64 = true;
+  }
+  if (fp32) {
+    if (!c->sval32) UFC_TRY(dalloc(c, &c->sval32, nv));
+    UFC_CUDA(c, cudaMemsetAsync(c->sval32, 0, sizeof(float) * nv, c->stream));
+    k_sym_pack<float><<<grid_for(c->N, 128), 128, 0, c->stream>>>(c->N, c->slice_ptr, c->uptr, c->brow, c->s_lcnt,
+                                                                  c->val64, c->sval32);
+    UFC_CUDA(c, cudaGetLastError());
+    c->has_sval32 = true;
+  }
+  release_graphs(c);
   return UFC_STATUS_OK;
 }
 

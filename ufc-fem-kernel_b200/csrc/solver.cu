@@ -107,6 +107,112 @@ __global__ void __launch_bounds__(kSpmvBlock)
   }
 }
 
+// y = K x from the symmetric storage: row i sums its upper blocks K_ij x_j
+// (j >= i, SELL-32, coalesced) and its lower blocks as transposes K_ji^T x_j of
+// the blocks stored by the earlier rows j.  Those transposed reads are from
+// blocks streamed by rows at most about one node plane earlier, so they come
+// from L2; the upper values are loaded with the default cache policy so that
+// they stay there.
+template <typename TV, typename TX, typename TA, int MODE>
+__global__ void __launch_bounds__(kSpmvBlock)
+    k_spmv_sym(int32_t N, int64_t nrows_pad, const int64_t* __restrict__ uptr, const int32_t* __restrict__ ucol,
+               const int64_t* __restrict__ lptr, const int32_t* __restrict__ lpos, const int32_t* __restrict__ lcol,
+               const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y,
+               CgScalars* __restrict__ scal, double* __restrict__ partials) {
+  if (MODE == kCg && scal->stop) return;
+  const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
+  double dot[1] = {0.0};
+  if (row < nrows_pad) {
+    const int64_t s = row >> 5;
+    const int t = (int)(row & 31);
+    TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
+    const int64_t ub = uptr[s], lb = lptr[s];
+    const int ulen = (int)((uptr[s + 1] - ub) >> 5);
+    const int llen = (int)((lptr[s + 1] - lb) >> 5);
+    const int32_t* ucp = ucol + ub + t;
+    const TV* uvp = val + 9 * ub + t;
+    const int32_t* lpp = lpos + lb + t;
+    const int32_t* lcp = lcol + lb + t;
+    // step j handles upper entry j and lower entry j, whose partners are read
+    // by the owning rows at about the same step; the common part has no
+    // branches so that the loads of both halves are in flight together
+    auto upper = [&](int j) {
+      const int64_t cj = __ldcs(ucp + 32 * j);
+      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
+      const TV* v = uvp + 288 * (int64_t)j;
+      a0 += (TA)v[0] * x0 + (TA)v[32] * x1 + (TA)v[64] * x2;
+      a1 += (TA)v[96] * x0 + (TA)v[128] * x1 + (TA)v[160] * x2;
+      a2 += (TA)v[192] * x0 + (TA)v[224] * x1 + (TA)v[256] * x2;
+    };
+    auto lower = [&](int j) {
+      const int64_t P = __ldcs(lpp + 32 * j);
+      const int64_t cj = __ldcs(lcp + 32 * j);
+      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
+      const TV* v = val + 9 * (P & ~int64_t(31)) + (P & 31);
+      // transposed block: (K_ji^T x)_r = sum_c K_ji[c][r] x_c
+      a0 += (TA)__ldg(v) * x0 + (TA)__ldg(v + 96) * x1 + (TA)__ldg(v + 192) * x2;
+      a1 += (TA)__ldg(v + 32) * x0 + (TA)__ldg(v + 128) * x1 + (TA)__ldg(v + 224) * x2;
+      a2 += (TA)__ldg(v + 64) * x0 + (TA)__ldg(v + 160) * x1 + (TA)__ldg(v + 256) * x2;
+    };
+    const int mlen = ulen < llen ? ulen : llen;
+    int j = 0;
+#pragma unroll 1
+    for (; j + 1 < mlen; j += 2) {
+      upper(j);
+      lower(j);
+      upper(j + 1);
+      lower(j + 1);
+    }
+    for (; j < mlen; ++j) {
+      upper(j);
+      lower(j);
+    }
+    for (int k = mlen; k < ulen; ++k) upper(k);
+    for (int k = mlen; k < llen; ++k) lower(k);
+    if (row < N) {
+      y[3 * row] = (TX)a0;
+      y[3 * row + 1] = (TX)a1;
+      y[3 * row + 2] = (TX)a2;
+      if (MODE == kCg)
+        dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
+    }
+  }
+  if (MODE == kCg) {
+    double tot[1];
+    if (grid_sum<1>(dot, partials, &scal->ticket[0], tot)) {
+      scal->pq = tot[0];
+      if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
+        scal->stop = 3;
+      } else {
+        scal->alpha = scal->rz / tot[0];
+      }
+    }
+  }
+}
+
+// 4 consecutive entries through 16-byte loads and stores (cudaMalloc bases are
+// 256-byte aligned; callers pass offsets that are multiples of 4 entries).
+template <typename T>
+__device__ __forceinline__ void ld4(const T* __restrict__ p, T (&o)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void st4(T* __restrict__ p, const T (&o)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+  } else {
+    *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+    *reinterpret_cast<double2*>(p + 2) = make_double2(o[2], o[3]);
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kVecBlock)
     k_cg_update(int64_t n, const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ r,
@@ -116,7 +222,29 @@ __global__ void __launch_bounds__(kVecBlock)
   const double alpha = scal->alpha;
   const T a = (T)alpha;
   T rz = T(0), rr = T(0);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t n4 = n >> 2;
+  for (int64_t k = gid; k < n4; k += stride) {
+    const int64_t i = k << 2;
+    T pv[4], qv[4], rv[4], dv[4];
+    double xv[4];
+    ld4(p + i, pv);
+    ld4(q + i, qv);
+    ld4(r + i, rv);
+    ld4(x + i, xv);
+    if (dinv) ld4(dinv + i, dv);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      xv[c] += alpha * (double)pv[c];
+      rv[c] -= a * qv[c];
+      const T zc = dinv ? dv[c] * rv[c] : rv[c];
+      rz += rv[c] * zc;
+      rr += rv[c] * rv[c];
+    }
+    st4(r + i, rv);
+    st4(x + i, xv);
+  }
+  for (int64_t i = (n4 << 2) + gid; i < n; i += stride) {
     const T pi = p[i], qi = q[i];
     x[i] += alpha * (double)pi;
     const T ri = r[i] - a * qi;
@@ -134,6 +262,7 @@ __global__ void __launch_bounds__(kVecBlock)
     scal->beta = tot[0] / rz_old;
     const int it = scal->iter + 1;
     scal->iter = it;
+    if (scal->hist && it <= scal->hist_cap) scal->hist[it - 1] = tot[1];
     if (tot[1] <= scal->tol2) scal->stop = 1;
     else if (!(fabs(rz_old) > 1e-300) || !isfinite(tot[0])) scal->stop = 3;
     else if (it >= scal->max_iter) scal->stop = 2;
@@ -147,7 +276,19 @@ __global__ void __launch_bounds__(kVecBlock)
                  const CgScalars* __restrict__ scal) {
   if (scal->stop) return;
   const T beta = (T)scal->beta;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t n4 = n >> 2;
+  for (int64_t k = gid; k < n4; k += stride) {
+    const int64_t i = k << 2;
+    T rv[4], pv[4], dv[4];
+    ld4(r + i, rv);
+    ld4(p + i, pv);
+    if (dinv) ld4(dinv + i, dv);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) pv[c] = (dinv ? dv[c] * rv[c] : rv[c]) + beta * pv[c];
+    st4(p + i, pv);
+  }
+  for (int64_t i = (n4 << 2) + gid; i < n; i += stride) {
     const T ri = r[i];
     p[i] = (dinv ? dinv[i] * ri : ri) + beta * p[i];
   }
@@ -199,12 +340,6 @@ __global__ void __launch_bounds__(kVecBlock)
   }
 }
 
-template <typename T>
-__global__ void k_zero(int64_t n, T* __restrict__ v) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    v[i] = T(0);
-}
-
 struct Run {
   Ctx* c;
   int prec;  // UFC_PRECISION_*
@@ -213,12 +348,14 @@ struct Run {
   int sg;    // SpMV grid
 };
 
-// CG vectors of type TX over stored values of type TV.
+// CG vectors of type TX over stored values of type TV; sym selects the
+// symmetric SpMV storage.
 template <typename TV, typename TX>
 struct Vecs {
   TX *r, *p, *q;
   const TV* val;
   const TX* dinv;
+  bool sym;
 };
 
 template <typename TV, typename TX>
@@ -231,16 +368,29 @@ Vecs<TV, TX> vecs(Ctx* c, bool precond) {
     v.r = c->r32; v.p = c->p32; v.q = c->q32;
     v.dinv = precond ? c->dinv32 : nullptr;
   }
-  if constexpr (sizeof(TV) == 8) v.val = c->val64;
-  else v.val = c->val32;
+  if constexpr (sizeof(TV) == 8) {
+    v.sym = c->has_sval64;
+    v.val = v.sym ? c->sval64 : c->val64;
+  } else {
+    v.sym = c->has_sval32;
+    v.val = v.sym ? c->sval32 : c->val32;
+  }
   return v;
+}
+
+template <typename TV, typename TX, typename TA, int MODE>
+void launch_spmv_sym(Ctx* c, int grid, cudaStream_t st, const TV* val, const TX* x, TX* y) {
+  k_spmv_sym<TV, TX, TA, MODE><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->uptr, c->ucol, c->lptr,
+                                                            c->lpos, c->lcol, val, x, y, c->scal, c->partials);
 }
 
 template <typename TV, typename TX, typename TA>
 void launch_iteration(const Run& R, const Vecs<TV, TX>& V, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
   Ctx* c = R.c;
   if (ev0) cudaEventRecord(ev0, st);
-  if (sizeof(TV) == 4 && c->val32_diff)
+  if (V.sym)
+    launch_spmv_sym<TV, TX, TA, kCg>(c, R.sg, st, V.val, V.p, V.q);
+  else if (sizeof(TV) == 4 && c->val32_diff)
     k_spmv<TV, TX, TA, kCg, true><<<R.sg, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col,
                                                                V.val, V.p, V.q, c->scal, c->partials);
   else
@@ -256,8 +406,11 @@ void launch_iteration(const Run& R, const Vecs<TV, TX>& V, cudaStream_t st, cuda
 int true_residual(const Run& R, bool want_bb) {
   Ctx* c = R.c;
   if (R.prec == UFC_PRECISION_FP64) {
-    k_spmv<double, double, double, kPlain, false><<<R.sg, kSpmvBlock, 0, c->stream>>>(
-        c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col, c->val64, c->x64, c->y64, nullptr, nullptr);
+    if (c->has_sval64)
+      launch_spmv_sym<double, double, double, kPlain>(c, R.sg, c->stream, c->sval64, c->x64, c->y64);
+    else
+      k_spmv<double, double, double, kPlain, false><<<R.sg, kSpmvBlock, 0, c->stream>>>(
+          c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col, c->val64, c->x64, c->y64, nullptr, nullptr);
     UFC_CUDA(c, cudaGetLastError());
     c->launches += 1;
   } else {
@@ -367,6 +520,14 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
     const double d = algo->refine_delta > 0.0 ? algo->refine_delta : 0.1;
     h.delta2 = d * d;
   }
+  // residual history (NM_Solver_State%residual_history): one double per iteration
+  const int32_t cap = std::min<int32_t>(h.max_iter, 1 << 20);
+  if (c->hist_cap < cap) {
+    UFC_TRY(dalloc(c, &c->hist, cap));
+    c->hist_cap = cap;
+  }
+  h.hist = c->hist;
+  h.hist_cap = c->hist_cap;
   UFC_CUDA(c, cudaMemcpyAsync(c->scal, &h, sizeof(CgScalars), cudaMemcpyHostToDevice, c->stream));
   UFC_TRY(true_residual(R, true));
   UFC_TRY(read_scalars(c));
@@ -518,6 +679,7 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   c->timing.kernel_launches = c->launches;
+  c->hist_len = std::min(c->h_scal->iter, c->hist_cap);
   st->niter = c->h_scal->iter;
   st->n_refine = n_refine;
   st->converged = converged ? 1 : 0;
@@ -544,6 +706,13 @@ int64_t spmv_bytes(const Ctx* c, int precision) {
   // block row pointers + x read once + y written once (slice padding excluded)
   const int64_t sv = precision == UFC_PRECISION_FP64 ? 8 : 4;  // stored value
   const int64_t sx = precision == UFC_PRECISION_FP32_REFINE ? 4 : 8;  // vector entry
+  const bool sym = precision == UFC_PRECISION_FP64 ? c->has_sval64 : c->has_sval32;
+  if (sym) {
+    // symmetric storage: upper blocks (values + column), lower references
+    // (position + column; their values are re-read from L2), x and y
+    const int64_t upper = (c->nnzb + c->N) / 2, lower = (c->nnzb - c->N) / 2;
+    return upper * (9 * sv + 4) + lower * 8 + 2 * c->n * sx;
+  }
   return c->nnzb * (9 * sv + 4) + 4 * ((int64_t)c->N + 1) + 2 * c->n * sx;
 }
 
@@ -553,11 +722,16 @@ int spmv(Ctx* c, int precision, const void* x, void* y) {
   const int64_t np = c->nslices * kSlice;
   if (precision == UFC_PRECISION_FP64) {
     if (!c->has_val64) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP64 values not assembled");
-    k_spmv<double, double, double, kPlain, false><<<sg, kSpmvBlock, 0, c->stream>>>(
-        c->N, np, c->slice_ptr, c->sell_col, c->val64, (const double*)x, (double*)y, nullptr, nullptr);
+    if (c->has_sval64)
+      launch_spmv_sym<double, double, double, kPlain>(c, sg, c->stream, c->sval64, (const double*)x, (double*)y);
+    else
+      k_spmv<double, double, double, kPlain, false><<<sg, kSpmvBlock, 0, c->stream>>>(
+          c->N, np, c->slice_ptr, c->sell_col, c->val64, (const double*)x, (double*)y, nullptr, nullptr);
   } else if (precision == UFC_PRECISION_FP32_REFINE) {
     if (!c->has_val32) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP32 values not assembled");
-    if (c->val32_diff)
+    if (c->has_sval32)
+      launch_spmv_sym<float, float, float, kPlain>(c, sg, c->stream, c->sval32, (const float*)x, (float*)y);
+    else if (c->val32_diff)
       k_spmv<float, float, float, kPlain, true><<<sg, kSpmvBlock, 0, c->stream>>>(
           c->N, np, c->slice_ptr, c->sell_col, c->val32, (const float*)x, (float*)y, nullptr, nullptr);
     else
@@ -565,7 +739,9 @@ int spmv(Ctx* c, int precision, const void* x, void* y) {
           c->N, np, c->slice_ptr, c->sell_col, c->val32, (const float*)x, (float*)y, nullptr, nullptr);
   } else if (precision == UFC_PRECISION_FP32_MATRIX) {
     if (!c->has_val32) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP32 values not assembled");
-    if (c->val32_diff)
+    if (c->has_sval32)
+      launch_spmv_sym<float, double, double, kPlain>(c, sg, c->stream, c->sval32, (const double*)x, (double*)y);
+    else if (c->val32_diff)
       k_spmv<float, double, double, kPlain, true><<<sg, kSpmvBlock, 0, c->stream>>>(
           c->N, np, c->slice_ptr, c->sell_col, c->val32, (const double*)x, (double*)y, nullptr, nullptr);
     else
@@ -613,8 +789,8 @@ int pcg_solve(Ctx* c, const double* b, double* x, const ufc_solver_algo* algo, u
   st->fp64_iters = 0;
   if (s == UFC_STATUS_NOT_CONVERGED && prec != UFC_PRECISION_FP64 && st->convergence_flag == 3 && c->has_val64 &&
       st->niter < algo->max_iter) {
-    // The FP32 matrix is too far from K for this problem (stall or divergence
-    // of the refined run): finish in FP64 from the best FP32 iterate.
+    // Stall or divergence of the refined FP32 run (the FP32 matrix is too far
+    // from K for this problem): finish in FP64 from the best FP32 iterate.
     ufc_solver_algo a64 = *algo;
     a64.precision_mode = UFC_PRECISION_FP64;
     a64.max_iter = algo->max_iter - st->niter;

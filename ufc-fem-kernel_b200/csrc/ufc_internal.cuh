@@ -33,6 +33,8 @@ struct CgScalars {
   int32_t stop;     // 1 converged (recursive), 2 max-iter, 3 breakdown
   int32_t want_update;
   double nr_rr, nr_ff, nr_ee;  // Newton: ||R_free||^2, ||F_int||^2, ||F_ext||^2
+  double* hist;        // ||r||^2 of the recursive residual per iteration (or null)
+  int32_t hist_cap;
   uint32_t ticket[8];  // last-block election counters, one per reduction site
 };
 
@@ -92,6 +94,20 @@ struct Ctx {
   double* dinv64 = nullptr;
   float* dinv32 = nullptr;
 
+  // symmetric SpMV storage: upper-triangle blocks (j >= i) in SELL-32, plus per
+  // row the positions of its lower blocks (stored transposed in earlier rows)
+  bool has_sym_pattern = false;
+  int64_t s_ublocks = 0, s_lblocks = 0;  // stored upper blocks (+ one zero slice), lower refs
+  int64_t* uptr = nullptr;               // [nslices+1]
+  int32_t* ucol = nullptr;               // [s_ublocks]
+  int64_t* lptr = nullptr;               // [nslices+1]
+  int32_t* lpos = nullptr;               // [s_lblocks] upper-storage position of block (j, i)
+  int32_t* lcol = nullptr;               // [s_lblocks] j
+  int32_t* s_lcnt = nullptr;             // [N] lower blocks per row (= position of the diagonal)
+  double* sval64 = nullptr;              // [(s_ublocks + 32) * 9]
+  float* sval32 = nullptr;
+  bool has_sval64 = false, has_sval32 = false;
+
   // Dirichlet set
   uint8_t* fixed = nullptr;  // [n]
   int32_t nfix = 0;
@@ -103,6 +119,8 @@ struct Ctx {
   float *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
   double* xb64 = nullptr;  // best iterate of an FP32 run (handed to the FP64 continuation)
   CgScalars* scal = nullptr;
+  double* hist = nullptr;       // residual history of the last solve (device)
+  int32_t hist_cap = 0, hist_len = 0;
   double* partials = nullptr;   // [partials_cap] per-block partial sums of grid reductions
   int64_t partials_cap = 0;
   CgScalars* h_scal = nullptr;  // pinned mirror
@@ -134,6 +152,8 @@ int check_dev_err(Ctx* c, const char* where);
 
 // pattern.cu
 int build_pattern(Ctx* c);
+int build_sym_pattern(Ctx* c);
+int pack_symmetric(Ctx* c, bool fp64, bool fp32);  // full SELL values -> symmetric SpMV copies
 int export_csr(Ctx* c, const ufc_csr_export_arg* a);
 
 // c3d8.cu

@@ -336,6 +336,14 @@ class FemModel:
         return {"spmv_launches": t.spmv_launches, "spmv_ms": t.spmv_ms, "spmv_bytes": t.spmv_bytes,
                 "precision": t.precision, "kernel_launches": t.kernel_launches}
 
+    def residual_history(self, max_len=1 << 20):
+        """||r_k||_2 of the CG recurrence per iteration of the last solve."""
+        out = np.zeros(max_len)
+        n = C.c_int32(0)
+        self._check(self.lib.ufc_last_residual_history(self.h, out.ctypes.data, int(max_len), C.byref(n)),
+                    "ufc_last_residual_history")
+        return out[: n.value].copy()
+
     # ---------------------------------------------------------------- nonlinear
     def nr_increment(self, u_prescribed, f_ext=None, max_iterations=25, tolerance_force=1e-8,
                      lin: SolverAlgo | None = None):
