@@ -202,3 +202,20 @@ def test_not_converged_and_errors(pkg):
     # the context stays usable after the failures
     m2 = _model(pkg, pkg.mesh.unit_cube_uniaxial())
     assert m2.solve(pkg.lifted_rhs(m2, m2.problem.f))[1].converged
+
+
+@pytest.mark.parametrize("nrhs", [1, 3, 16])
+def test_block_solve_matches_single(pkg, orc, nrhs):
+    p = pkg.mesh.density_problem(10, 5, 5, seed=5, n_rhs=max(nrhs, 1))
+    m = _model(pkg, p, pkg.BUILD_FP64)
+    F = np.ascontiguousarray(p.meta["F"][:nrhs])
+    algo = pkg.SolverAlgo(tolerance=1e-10)
+    X, states = m.solve_block(F, algo)
+    K = orc.Model(p).assemble()
+    for k in range(nrhs):
+        assert states[k].converged and states[k].rnorm <= 1e-10
+        r = F[k] - K.matvec(X[k])
+        assert np.linalg.norm(r) / np.linalg.norm(F[k]) <= 2e-10
+        x1, s1 = m.solve(F[k], algo)
+        assert np.linalg.norm(X[k] - x1) <= 1e-8 * np.linalg.norm(x1)
+        assert abs(states[k].niter - s1.niter) <= 2
