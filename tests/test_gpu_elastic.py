@@ -204,7 +204,7 @@ def test_not_converged_and_errors(pkg):
     assert m2.solve(pkg.lifted_rhs(m2, m2.problem.f))[1].converged
 
 
-@pytest.mark.parametrize("nrhs", [1, 3, 16])
+@pytest.mark.parametrize("nrhs", [1, 2, 3, 8, 16, 32])
 def test_block_solve_matches_single(pkg, orc, nrhs):
     p = pkg.mesh.density_problem(10, 5, 5, seed=5, n_rhs=max(nrhs, 1))
     m = _model(pkg, p, pkg.BUILD_FP64)

@@ -53,6 +53,25 @@ def test_nr_increments_match_oracle(pkg, orc):
     np.testing.assert_allclose(epeq.ravel(), state["epeq"], rtol=1e-6)
 
 
+def test_nr_increments_fp32_refined_inner_solves(pkg, orc):
+    """FP32 CG on the tangent rounded from its FP64 assembly, refined with the
+    FP64 tangent residual, reaches the same Newton iterates as the oracle."""
+    p = pkg.mesh.j2_bar(6, 3, 3)
+    steps, strain = 5, 0.006
+    targets = [pkg.mesh.j2_bar_target(p, s, n_steps=steps, strain=strain) for s in range(1, steps + 1)]
+    hist, state, _ = orc.nr_j2(orc.Model(p), targets)
+    m = _bar_model(pkg, p)
+    lin = pkg.SolverAlgo(tolerance=1e-12, precision_mode=pkg.PRECISION_FP32_REFINE)
+    for s, tgt in enumerate(targets):
+        res = m.nr_increment(tgt, tolerance_force=1e-8, lin=lin)
+        assert res.converged and res.iterations <= 8
+        m.commit()
+        np.testing.assert_allclose(m.displacement(), hist[s], rtol=0, atol=1e-8 * np.abs(hist[s]).max())
+    epeq, sig, _ = m.j2_state()
+    np.testing.assert_allclose(sig.reshape(-1, 6), state["sig"].reshape(-1, 6), rtol=0,
+                               atol=1e-7 * np.abs(state["sig"]).max())
+
+
 def test_rollback_restores_committed_state(pkg):
     p = pkg.mesh.j2_bar(3, 2, 2)
     m = _bar_model(pkg, p)

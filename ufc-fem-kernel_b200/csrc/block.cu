@@ -4,13 +4,17 @@
 //
 // Vectors are interleaved, entry (dof i, rhs k) at i*nr + k with nr the number
 // of right-hand sides rounded up to a power of two (<= 32; padded columns are
-// zero and inactive).  One thread handles one (block row, rhs) pair of the
-// SpMV: the nr threads of a row read the same matrix values (one request per
-// warp) and consecutive x entries.  Each right-hand side has its own
-// alpha, beta and stop test; a converged right-hand side is frozen (alpha =
-// beta = 0) while the others continue.  Reductions are per right-hand side and
-// deterministic: lanes that hold the same rhs are combined by shuffles, then
-// across warps and blocks in a fixed order.
+// zero and inactive).  A thread owns G = min(nr, 8) consecutive right-hand
+// sides of one block row: it loads each stored 3x3 block once (the threads of
+// a warp cover 32/tpr consecutive rows of a SELL slice, tpr = nr/G threads per
+// row, so every value load is one coalesced line) and the G entries of each x
+// component with 16-byte loads, keeping 3*G row sums in registers.  The vector
+// kernels give every thread the same G right-hand sides of successive dofs.
+// Each right-hand side has its own alpha, beta and stop test; a converged
+// right-hand side is frozen (alpha = beta = 0) while the others continue.
+// Reductions are per right-hand side and deterministic: lanes that hold the
+// same right-hand sides are combined by shuffles, then warps and blocks in a
+// fixed order.  Batches of iterations run as one CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,6 +30,8 @@ namespace {
 
 constexpr int kMaxRhs = 32;
 constexpr int kBlk = 256;
+constexpr int kWarps = kBlk / 32;
+constexpr int kNvMax = 3;
 
 struct BScalars {
   double rz[kMaxRhs], rz_old[kMaxRhs], alpha[kMaxRhs], beta[kMaxRhs], rr[kMaxRhs], tol2[kMaxRhs];
@@ -37,28 +43,73 @@ struct BScalars {
   uint32_t ticket[4];
 };
 
-// Sum NV values per rhs over the grid; the rhs of a thread is threadIdx.x % nr
-// for every element it touches (block size and grid stride are multiples of
-// nr).  Returns true in the threads k < nr of the last block, with out[v] the
-// total of value v for rhs k.
-template <int NV>
-__device__ bool group_grid_sum(double (&v)[NV], int nr, double* __restrict__ partials, uint32_t* ticket,
-                               double (&out)[NV]) {
-  __shared__ double sh[kBlk / 32][NV][kMaxRhs];
-  __shared__ double fin[kBlk][NV];
+// G consecutive doubles (16-byte aligned when G >= 2).
+template <int G>
+__device__ __forceinline__ void ldg_g(const double* __restrict__ p, double (&o)[G]) {
+  if constexpr (G == 1) {
+    o[0] = __ldg(p);
+  } else {
+#pragma unroll
+    for (int i = 0; i < G; i += 2) {
+      const double2 v = __ldg(reinterpret_cast<const double2*>(p + i));
+      o[i] = v.x;
+      o[i + 1] = v.y;
+    }
+  }
+}
+
+template <int G>
+__device__ __forceinline__ void ld_g(const double* p, double (&o)[G]) {
+  if constexpr (G == 1) {
+    o[0] = *p;
+  } else {
+#pragma unroll
+    for (int i = 0; i < G; i += 2) {
+      const double2 v = *reinterpret_cast<const double2*>(p + i);
+      o[i] = v.x;
+      o[i + 1] = v.y;
+    }
+  }
+}
+
+template <int G>
+__device__ __forceinline__ void st_g(double* p, const double (&o)[G]) {
+  if constexpr (G == 1) {
+    *p = o[0];
+  } else {
+#pragma unroll
+    for (int i = 0; i < G; i += 2) *reinterpret_cast<double2*>(p + i) = make_double2(o[i], o[i + 1]);
+  }
+}
+
+// Per-rhs grid sum.  Thread t holds v[q][i] for rhs (t % tpr)*G + i; lanes with
+// the same t % tpr are combined by shuffles, then the warps of the block in
+// order, then the blocks in order by the last block to finish.  Returns true
+// in the threads k < nr of that block, out[q] being the total of value q for
+// rhs k; the ticket is reset for the next launch.
+template <int G, int NV>
+__device__ bool rhs_grid_sum(double (&v)[NV][G], int tpr, int nr, double* __restrict__ partials, uint32_t* ticket,
+                             double (&out)[NV]) {
+  __shared__ double sh[kWarps][NV][kMaxRhs];
+  __shared__ double fin[kBlk * NV];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int o = 16; o >= nr; o >>= 1)
+  for (int o = 16; o >= tpr; o >>= 1)
 #pragma unroll
-    for (int q = 0; q < NV; ++q) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
-  if (lane < nr)
+    for (int q = 0; q < NV; ++q)
 #pragma unroll
-    for (int q = 0; q < NV; ++q) sh[w][q][lane] = v[q];
+      for (int i = 0; i < G; ++i) v[q][i] += __shfl_down_sync(0xffffffffu, v[q][i], o);
+  if (lane < tpr)
+#pragma unroll
+    for (int q = 0; q < NV; ++q)
+#pragma unroll
+      for (int i = 0; i < G; ++i) sh[w][q][lane * G + i] = v[q][i];
   __syncthreads();
   if (threadIdx.x < nr) {
+#pragma unroll
     for (int q = 0; q < NV; ++q) {
       double s = 0.0;
-      for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) s += sh[ww][q][threadIdx.x];
+      for (int ww = 0; ww < kWarps; ++ww) s += sh[ww][q][threadIdx.x];
       partials[((int64_t)blockIdx.x * NV + q) * kMaxRhs + threadIdx.x] = s;
     }
   }
@@ -69,21 +120,21 @@ __device__ bool group_grid_sum(double (&v)[NV], int nr, double* __restrict__ par
   if (!last) return false;
   __threadfence();
   // last block: thread t sums the blocks b = t/nr (mod blockDim/nr) for rhs t % nr
-  const int k = threadIdx.x % nr, per = blockDim.x / nr;
+  const int k = threadIdx.x % nr, gi = threadIdx.x / nr, groups = kBlk / nr;
   double acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-  for (int64_t b = threadIdx.x / nr; b < gridDim.x; b += per)
+  for (int64_t b = gi; b < gridDim.x; b += groups)
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] += __ldcg(partials + (b * NV + q) * kMaxRhs + k);
 #pragma unroll
-  for (int q = 0; q < NV; ++q) fin[threadIdx.x][q] = acc[q];
+  for (int q = 0; q < NV; ++q) fin[(gi * NV + q) * nr + k] = acc[q];
   __syncthreads();
   if (threadIdx.x < nr) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       double s = 0.0;
-      for (int g = 0; g < per; ++g) s += fin[g * nr + threadIdx.x][q];
+      for (int g = 0; g < groups; ++g) s += fin[(g * NV + q) * nr + threadIdx.x];
       out[q] = s;
     }
     if (threadIdx.x == 0) *ticket = 0u;
@@ -92,44 +143,70 @@ __device__ bool group_grid_sum(double (&v)[NV], int nr, double* __restrict__ par
   return false;
 }
 
-// y = K x for nr interleaved vectors (FP64 SELL values); mode 1 also forms
-// p.q per rhs and alpha.
-template <int MODE>
-__global__ void __launch_bounds__(kBlk)
-    k_bspmv(int32_t N, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
-            const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y, int nr,
+// y = K x for nr interleaved vectors (FP64 SELL values); MODE 1 also forms
+// p.q per rhs and alpha.  One warp task = 32/tpr rows of a slice.
+template <int G, int MODE>
+__global__ void __launch_bounds__(kBlk, 2)
+    k_bspmv(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
+            const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y, int nr, int tpr,
             BScalars* __restrict__ s, double* __restrict__ partials) {
   if (MODE == 1 && s->stop) return;
-  const int k = threadIdx.x % nr;
-  const int64_t units = (int64_t)N * nr;
-  double dot[1] = {0.0};
-  for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < units; u += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = u / nr;
-    const int64_t sl = row >> 5;
-    const int t = (int)(row & 31);
+  const int lane = threadIdx.x & 31;
+  const int rpw = 32 / tpr;
+  const int rl = lane / tpr;
+  const int k0 = (lane % tpr) * G;
+  double dot[1][G];
+#pragma unroll
+  for (int i = 0; i < G; ++i) dot[0][i] = 0.0;
+  const int64_t tasks = nslices * tpr;
+  const int64_t wstride = ((int64_t)gridDim.x * kBlk) >> 5;
+  for (int64_t task = ((int64_t)blockIdx.x * kBlk + threadIdx.x) >> 5; task < tasks; task += wstride) {
+    const int64_t sl = task / tpr;
+    const int t = (int)(task % tpr) * rpw + rl;
+    const int64_t row = sl * kSlice + t;
     const int64_t base = sptr[sl];
     const int len = (int)((sptr[sl + 1] - base) >> 5);
     const int32_t* cp = col + base + t;
     const double* vp = val + 9 * base + t;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    double acc[3][G];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int i = 0; i < G; ++i) acc[r][i] = 0.0;
     for (int j = 0; j < len; ++j) {
-      const int64_t cj = cp[32 * j];
-      const double x0 = __ldg(x + (3 * cj) * nr + k), x1 = __ldg(x + (3 * cj + 1) * nr + k),
-                   x2 = __ldg(x + (3 * cj + 2) * nr + k);
+      const int64_t cj = __ldcs(cp + 32 * j);
       const double* v = vp + 288 * (int64_t)j;
-      a0 += v[0] * x0 + v[32] * x1 + v[64] * x2;
-      a1 += v[96] * x0 + v[128] * x1 + v[160] * x2;
-      a2 += v[192] * x0 + v[224] * x1 + v[256] * x2;
+      double m[9];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) m[c] = __ldcs(v + 32 * c);
+#pragma unroll
+      for (int comp = 0; comp < 3; ++comp) {
+        double xv[G];
+        ldg_g<G>(x + (3 * cj + comp) * nr + k0, xv);
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+          acc[0][i] += m[comp] * xv[i];
+          acc[1][i] += m[3 + comp] * xv[i];
+          acc[2][i] += m[6 + comp] * xv[i];
+        }
+      }
     }
-    y[(3 * row) * nr + k] = a0;
-    y[(3 * row + 1) * nr + k] = a1;
-    y[(3 * row + 2) * nr + k] = a2;
-    if (MODE == 1)
-      dot[0] += x[(3 * row) * nr + k] * a0 + x[(3 * row + 1) * nr + k] * a1 + x[(3 * row + 2) * nr + k] * a2;
+    if (row < N) {
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        st_g<G>(y + (3 * row + r) * nr + k0, acc[r]);
+        if (MODE == 1) {
+          double xr[G];
+          ldg_g<G>(x + (3 * row + r) * nr + k0, xr);
+#pragma unroll
+          for (int i = 0; i < G; ++i) dot[0][i] += xr[i] * acc[r][i];
+        }
+      }
+    }
   }
   if (MODE == 1) {
     double tot[1];
-    if (group_grid_sum<1>(dot, nr, partials, &s->ticket[0], tot)) {
+    if (rhs_grid_sum<G, 1>(dot, tpr, nr, partials, &s->ticket[0], tot)) {
       const int kk = threadIdx.x;
       const bool ok = s->active[kk] && fabs(tot[0]) > 1e-300 && isfinite(tot[0]);
       s->alpha[kk] = ok ? s->rz[kk] / tot[0] : 0.0;
@@ -138,24 +215,42 @@ __global__ void __launch_bounds__(kBlk)
   }
 }
 
+// x += alpha p, r -= alpha q, then r.z and r.r per rhs, beta and the stop tests.
+template <int G>
 __global__ void __launch_bounds__(kBlk)
-    k_bupdate(int64_t nn, int nr, const double* __restrict__ p, const double* __restrict__ q, double* __restrict__ r,
-              double* __restrict__ x, const double* __restrict__ dinv, BScalars* __restrict__ s,
-              double* __restrict__ partials) {
+    k_bupdate(int64_t n, int nr, int tpr, const double* __restrict__ p, const double* __restrict__ q,
+              double* __restrict__ r, double* __restrict__ x, const double* __restrict__ dinv,
+              BScalars* __restrict__ s, double* __restrict__ partials) {
   if (s->stop) return;
-  const int k = threadIdx.x % nr;
-  const double a = s->alpha[k];
-  double v[2] = {0.0, 0.0};
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
-    x[e] += a * p[e];
-    const double re = r[e] - a * q[e];
-    r[e] = re;
-    const double ze = dinv ? dinv[e / nr] * re : re;
-    v[0] += re * ze;
-    v[1] += re * re;
+  const int64_t tid = (int64_t)blockIdx.x * kBlk + threadIdx.x, stride = (int64_t)gridDim.x * kBlk;
+  const int k0 = (int)(tid % tpr) * G;
+  double a[G];
+#pragma unroll
+  for (int i = 0; i < G; ++i) a[i] = s->alpha[k0 + i];
+  double v[2][G];
+#pragma unroll
+  for (int i = 0; i < G; ++i) v[0][i] = v[1][i] = 0.0;
+  const int64_t groups = n * tpr;
+  for (int64_t idx = tid; idx < groups; idx += stride) {
+    const int64_t e = idx * G;
+    const double d = dinv ? __ldg(dinv + idx / tpr) : 1.0;
+    double pv[G], qv[G], rv[G], xv[G];
+    ldg_g<G>(p + e, pv);
+    ldg_g<G>(q + e, qv);
+    ld_g<G>(r + e, rv);
+    ld_g<G>(x + e, xv);
+#pragma unroll
+    for (int i = 0; i < G; ++i) {
+      xv[i] += a[i] * pv[i];
+      rv[i] -= a[i] * qv[i];
+      v[0][i] += rv[i] * (d * rv[i]);
+      v[1][i] += rv[i] * rv[i];
+    }
+    st_g<G>(r + e, rv);
+    st_g<G>(x + e, xv);
   }
   double tot[2];
-  if (group_grid_sum<2>(v, nr, partials, &s->ticket[1], tot)) {
+  if (rhs_grid_sum<G, 2>(v, tpr, nr, partials, &s->ticket[1], tot)) {
     const int kk = threadIdx.x;
     if (s->active[kk]) {
       s->rz_old[kk] = s->rz[kk];
@@ -182,35 +277,65 @@ __global__ void __launch_bounds__(kBlk)
   }
 }
 
+// p = D^-1 r + beta p for the rhs still active.
+template <int G>
 __global__ void __launch_bounds__(kBlk)
-    k_bpupdate(int64_t nn, int nr, const double* __restrict__ r, const double* __restrict__ dinv,
+    k_bpupdate(int64_t n, int nr, int tpr, const double* __restrict__ r, const double* __restrict__ dinv,
                double* __restrict__ p, const BScalars* __restrict__ s) {
   if (s->stop) return;
-  const int k = threadIdx.x % nr;
-  const double b = s->beta[k];
-  const bool act = s->active[k];
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
-    if (!act) continue;
-    const double re = r[e];
-    p[e] = (dinv ? dinv[e / nr] * re : re) + b * p[e];
+  const int64_t tid = (int64_t)blockIdx.x * kBlk + threadIdx.x, stride = (int64_t)gridDim.x * kBlk;
+  const int k0 = (int)(tid % tpr) * G;
+  double b[G];
+  bool act[G], any = false;
+#pragma unroll
+  for (int i = 0; i < G; ++i) {
+    b[i] = s->beta[k0 + i];
+    act[i] = s->active[k0 + i] != 0;
+    any |= act[i];
+  }
+  if (!any) return;
+  const int64_t groups = n * tpr;
+  for (int64_t idx = tid; idx < groups; idx += stride) {
+    const int64_t e = idx * G;
+    const double d = dinv ? __ldg(dinv + idx / tpr) : 1.0;
+    double rv[G], pv[G];
+    ldg_g<G>(r + e, rv);
+    ld_g<G>(p + e, pv);
+#pragma unroll
+    for (int i = 0; i < G; ++i)
+      if (act[i]) pv[i] = d * rv[i] + b[i] * pv[i];
+    st_g<G>(p + e, pv);
   }
 }
 
 // r = b - y with ||r||^2, ||b||^2 and r.z per rhs (the state a restart needs).
+template <int G>
 __global__ void __launch_bounds__(kBlk)
-    k_bresid(int64_t nn, int nr, const double* __restrict__ b, const double* __restrict__ y, double* __restrict__ r,
-             const double* __restrict__ dinv, BScalars* __restrict__ s, double* __restrict__ partials) {
-  double v[3] = {0.0, 0.0, 0.0};
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
-    const double be = b[e];
-    const double re = be - y[e];
-    r[e] = re;
-    v[0] += re * re;
-    v[1] += be * be;
-    v[2] += re * (dinv ? dinv[e / nr] * re : re);
+    k_bresid(int64_t n, int nr, int tpr, const double* __restrict__ bv, const double* __restrict__ y,
+             double* __restrict__ r, const double* __restrict__ dinv, BScalars* __restrict__ s,
+             double* __restrict__ partials) {
+  const int64_t tid = (int64_t)blockIdx.x * kBlk + threadIdx.x, stride = (int64_t)gridDim.x * kBlk;
+  double v[3][G];
+#pragma unroll
+  for (int i = 0; i < G; ++i) v[0][i] = v[1][i] = v[2][i] = 0.0;
+  const int64_t groups = n * tpr;
+  for (int64_t idx = tid; idx < groups; idx += stride) {
+    const int64_t e = idx * G;
+    const double d = dinv ? __ldg(dinv + idx / tpr) : 1.0;
+    double be[G], ye[G], re[G];
+    ldg_g<G>(bv + e, be);
+    ldg_g<G>(y + e, ye);
+#pragma unroll
+    for (int i = 0; i < G; ++i) {
+      re[i] = be[i] - ye[i];
+      v[0][i] += re[i] * re[i];
+      v[1][i] += be[i] * be[i];
+      v[2][i] += re[i] * (d * re[i]);
+    }
+    st_g<G>(r + e, re);
   }
   double tot[3];
-  if (group_grid_sum<3>(v, nr, partials, &s->ticket[2], tot)) {
+  if (rhs_grid_sum<G, 3>(v, tpr, nr, partials, &s->ticket[2], tot)) {
     const int kk = threadIdx.x;
     s->true_rr[kk] = tot[0];
     s->bb[kk] = tot[1];
@@ -244,84 +369,73 @@ __global__ void k_deinterleave(int64_t n, int nrhs, int nr, const double* __rest
   }
 }
 
-int grid_vec(int64_t units) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (int)std::max<int64_t>(1, std::min<int64_t>((units + kBlk - 1) / kBlk, (int64_t)sms * 8));
+int sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+// blocks for `threads` grid-stride threads, at most 8 per SM
+int grid_blocks(int64_t threads) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((threads + kBlk - 1) / kBlk, (int64_t)sm_count() * 8));
+}
+
+struct BlockRun {
+  Ctx* c;
+  int nr, tpr;
+  int64_t n, nn;
+  const double* dinv;
+  double *bx, *xx, *rx, *px, *qx;
+  BScalars* s;
+  double* partials;
+  int g_spmv, g_vec;
+};
+
+template <int G>
+void launch_bspmv(const BlockRun& B, cudaStream_t st, int mode, const double* x, double* y) {
+  Ctx* c = B.c;
+  if (mode == 1)
+    k_bspmv<G, 1><<<B.g_spmv, kBlk, 0, st>>>(c->N, c->nslices, c->slice_ptr, c->sell_col, c->val64, x, y, B.nr,
+                                              B.tpr, B.s, B.partials);
+  else
+    k_bspmv<G, 0><<<B.g_spmv, kBlk, 0, st>>>(c->N, c->nslices, c->slice_ptr, c->sell_col, c->val64, x, y, B.nr,
+                                              B.tpr, B.s, B.partials);
+}
+
+template <int G>
+void launch_biteration(const BlockRun& B, cudaStream_t st) {
+  launch_bspmv<G>(B, st, 1, B.px, B.qx);
+  k_bupdate<G><<<B.g_vec, kBlk, 0, st>>>(B.n, B.nr, B.tpr, B.px, B.qx, B.rx, B.xx, B.dinv, B.s, B.partials);
+  k_bpupdate<G><<<B.g_vec, kBlk, 0, st>>>(B.n, B.nr, B.tpr, B.rx, B.dinv, B.px, B.s);
+}
+
+template <int G>
+void launch_bresidual(const BlockRun& B, cudaStream_t st) {
+  launch_bspmv<G>(B, st, 0, B.xx, B.qx);
+  k_bresid<G><<<B.g_vec, kBlk, 0, st>>>(B.n, B.nr, B.tpr, B.bx, B.qx, B.rx, B.dinv, B.s, B.partials);
 }
 
 }  // namespace
 
-int pcg_solve_block(Ctx* c, int nrhs, const double* B, double* X, const ufc_solver_algo* algo,
-                    ufc_solver_state* st) {
-  if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: pattern not built");
-  if (nrhs < 1 || nrhs > kMaxRhs) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: nrhs must be 1..32");
-  if (algo->precision_mode != UFC_PRECISION_FP64)
-    return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve_block: FP64 only");
-  if (!c->has_val64) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: FP64 values not assembled");
-  if (algo->method != UFC_SOLV_METHOD_CG || algo->max_iter <= 0)
-    return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: method must be CG and max_iter > 0");
-  int nr = 1;
-  while (nr < nrhs) nr <<= 1;
-  const int64_t nn = c->n * nr;
-  const double* dinv = algo->precond_type == UFC_SOLV_PREC_JACOBI ? c->dinv64 : nullptr;
-  double *bx = nullptr, *xx = nullptr, *rx = nullptr, *px = nullptr, *qx = nullptr;
-  BScalars* s = nullptr;
-  BScalars* hs = nullptr;
-  double* partials = nullptr;
-  int32_t* restart_dev = nullptr;
-  const int gv = grid_vec(nn);
-  auto cleanup = [&]() {
-    dfree(&bx); dfree(&xx); dfree(&rx); dfree(&px); dfree(&qx); dfree(&s); dfree(&partials); dfree(&restart_dev);
-    if (hs) cudaFreeHost(hs);
-    hs = nullptr;
-  };
-  int status = UFC_STATUS_OK;
-#define BTRY(expr)            \
-  do {                        \
-    status = (expr);          \
-    if (status != UFC_STATUS_OK) { cleanup(); return status; } \
-  } while (0)
-#define BCUDA(expr)                                                   \
-  do {                                                                \
-    cudaError_t _e = (expr);                                          \
-    if (_e != cudaSuccess) { cleanup(); return cuda_fail(c, _e, #expr); } \
-  } while (0)
-  BTRY(dalloc(c, &bx, nn));
-  BTRY(dalloc(c, &xx, nn));
-  BTRY(dalloc(c, &rx, nn));
-  BTRY(dalloc(c, &px, nn));
-  BTRY(dalloc(c, &qx, nn));
-  BTRY(dalloc(c, &s, 1));
-  BTRY(dalloc(c, &partials, (int64_t)gv * 3 * kMaxRhs));
-  BTRY(dalloc(c, &restart_dev, kMaxRhs));
-  BCUDA(cudaMallocHost((void**)&hs, sizeof(BScalars)));
-  cudaEvent_t t0, t1;
-  BCUDA(cudaEventCreate(&t0));
-  BCUDA(cudaEventCreate(&t1));
-  BCUDA(cudaEventRecord(t0, c->stream));
-
-  k_interleave<<<gv, kBlk, 0, c->stream>>>(c->n, nrhs, nr, B, bx);
-  if (algo->use_x0)
-    k_interleave<<<gv, kBlk, 0, c->stream>>>(c->n, nrhs, nr, X, xx);
-  else
-    BCUDA(cudaMemsetAsync(xx, 0, sizeof(double) * nn, c->stream));
-  BScalars h{};
-  h.nr = nr;
-  h.max_iter = algo->max_iter;
-  BCUDA(cudaMemcpyAsync(s, &h, sizeof(BScalars), cudaMemcpyHostToDevice, c->stream));
-
+template <int G>
+static int pcg_block_run(BlockRun& B, int nrhs, const ufc_solver_algo* algo, BScalars* hs, int32_t* restart_dev,
+                         std::vector<double>& bnorm, std::vector<double>& tol, std::vector<int>& n_refine,
+                         ufc_solver_state* st) {
+  Ctx* c = B.c;
+  const int nr = B.nr;
   auto residual = [&]() -> int {
-    k_bspmv<0><<<gv, kBlk, 0, c->stream>>>(c->N, c->slice_ptr, c->sell_col, c->val64, xx, qx, nr, s, partials);
-    k_bresid<<<gv, kBlk, 0, c->stream>>>(nn, nr, bx, qx, rx, dinv, s, partials);
+    launch_bresidual<G>(B, c->stream);
     UFC_CUDA(c, cudaGetLastError());
-    UFC_CUDA(c, cudaMemcpyAsync(hs, s, sizeof(BScalars), cudaMemcpyDeviceToHost, c->stream));
+    c->launches += 2;
+    UFC_CUDA(c, cudaMemcpyAsync(hs, B.s, sizeof(BScalars), cudaMemcpyDeviceToHost, c->stream));
     UFC_CUDA(c, cudaStreamSynchronize(c->stream));
     return UFC_STATUS_OK;
   };
-  BTRY(residual());
-  std::vector<double> tol(nr, 0.0), bnorm(nr, 1.0);
+  UFC_TRY(residual());
   for (int k = 0; k < nr; ++k) {
     const double bn = std::sqrt(hs->bb[k]);
     bnorm[k] = bn < 1e-30 ? 1.0 : bn;
@@ -329,15 +443,24 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* B, double* X, const ufc_solv
     if (k < nrhs) st[k].initial_residual = std::sqrt(hs->true_rr[k]);
   }
   const int batch = algo->check_every > 0 ? algo->check_every : 32;
+  // one graph of `batch` iterations, launched until every rhs stops
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  UFC_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  for (int b = 0; b < batch; ++b) launch_biteration<G>(B, c->stream);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+  BScalars h{};
   std::vector<int32_t> restart(kMaxRhs, 0);
-  std::vector<int> conv(nr, 0), n_refine(nr, 0);
-  int total_iter = 0;
-  for (int round = 0; round < 64; ++round) {
+  int total_iter = 0, status = UFC_STATUS_OK;
+  for (int round = 0; round < 64 && status == UFC_STATUS_OK; ++round) {
     // (re)start every rhs whose FP64 residual is above its tolerance
     bool any = false;
     for (int k = 0; k < nr; ++k) {
       const bool ok = k >= nrhs || std::sqrt(hs->true_rr[k]) <= tol[k];
-      conv[k] = ok;
       restart[k] = ok ? 0 : 1;
       any |= !ok;
       h.tol2[k] = tol[k] * tol[k];
@@ -352,35 +475,122 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* B, double* X, const ufc_solv
     h.max_iter = algo->max_iter - total_iter;
     h.nr = nr;
     for (int q = 0; q < 4; ++q) h.ticket[q] = 0;
-    cudaMemcpyAsync(s, &h, sizeof(BScalars), cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(B.s, &h, sizeof(BScalars), cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(restart_dev, restart.data(), sizeof(int32_t) * kMaxRhs, cudaMemcpyHostToDevice, c->stream);
-    k_bpinit<<<gv, kBlk, 0, c->stream>>>(nn, nr, rx, dinv, px, restart_dev);
-    // iterate in batches until every active rhs stops
+    k_bpinit<<<grid_blocks(B.nn), kBlk, 0, c->stream>>>(B.nn, nr, B.rx, B.dinv, B.px, restart_dev);
+    c->launches += 1;
     for (;;) {
-      for (int b = 0; b < batch; ++b) {
-        k_bspmv<1><<<gv, kBlk, 0, c->stream>>>(c->N, c->slice_ptr, c->sell_col, c->val64, px, qx, nr, s, partials);
-        k_bupdate<<<gv, kBlk, 0, c->stream>>>(nn, nr, px, qx, rx, xx, dinv, s, partials);
-        k_bpupdate<<<gv, kBlk, 0, c->stream>>>(nn, nr, rx, dinv, px, s);
+      e = cudaGraphLaunch(ge, c->stream);
+      if (e != cudaSuccess) {
+        status = cuda_fail(c, e, "cudaGraphLaunch");
+        break;
       }
-      cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess) { cleanup(); return cuda_fail(c, e, "ufc_pcg_solve_block"); }
-      cudaMemcpyAsync(hs, s, sizeof(BScalars), cudaMemcpyDeviceToHost, c->stream);
-      cudaStreamSynchronize(c->stream);
+      c->launches += 3 * (int64_t)batch;
+      cudaMemcpyAsync(hs, B.s, sizeof(BScalars), cudaMemcpyDeviceToHost, c->stream);
+      e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess) {
+        status = cuda_fail(c, e, "ufc_pcg_solve_block");
+        break;
+      }
       if (hs->stop) break;
     }
+    if (status != UFC_STATUS_OK) break;
     total_iter += hs->iter;
-    for (int k = 0; k < nr; ++k) h.iters[k] = hs->iters[k];
+    const int stop = hs->stop;
     // FP64 true residual of every rhs (residual replacement)
     const std::vector<int32_t> iters_keep(hs->iters, hs->iters + kMaxRhs);
-    BTRY(residual());
+    status = residual();
+    if (status != UFC_STATUS_OK) break;
     for (int k = 0; k < nr; ++k) {
       hs->iters[k] = iters_keep[k];
       ++n_refine[k];
     }
-    if (hs->stop == 2) break;
+    if (stop == 2) break;
+  }
+  cudaGraphExecDestroy(ge);
+  return status;
+}
+
+int pcg_solve_block(Ctx* c, int nrhs, const double* Bm, double* X, const ufc_solver_algo* algo,
+                    ufc_solver_state* st) {
+  if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: pattern not built");
+  if (nrhs < 1 || nrhs > kMaxRhs) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: nrhs must be 1..32");
+  if (algo->precision_mode != UFC_PRECISION_FP64)
+    return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve_block: FP64 only");
+  if (!c->has_val64) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: FP64 values not assembled");
+  if (algo->method != UFC_SOLV_METHOD_CG || algo->max_iter <= 0)
+    return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: method must be CG and max_iter > 0");
+  int nr = 1;
+  while (nr < nrhs) nr <<= 1;
+  const int G = std::min(nr, 8);
+  BlockRun B{};
+  B.c = c;
+  B.nr = nr;
+  B.tpr = nr / G;
+  B.n = c->n;
+  B.nn = c->n * nr;
+  B.dinv = algo->precond_type == UFC_SOLV_PREC_JACOBI ? c->dinv64 : nullptr;
+  B.g_spmv = grid_blocks(c->nslices * B.tpr * 32);
+  B.g_vec = grid_blocks(c->n * B.tpr);
+  BScalars* hs = nullptr;
+  int32_t* restart_dev = nullptr;
+  auto cleanup = [&]() {
+    dfree(&B.bx); dfree(&B.xx); dfree(&B.rx); dfree(&B.px); dfree(&B.qx); dfree(&B.s); dfree(&B.partials);
+    dfree(&restart_dev);
+    if (hs) cudaFreeHost(hs);
+    hs = nullptr;
+  };
+  int status = UFC_STATUS_OK;
+#define BTRY(expr)            \
+  do {                        \
+    status = (expr);          \
+    if (status != UFC_STATUS_OK) { cleanup(); return status; } \
+  } while (0)
+#define BCUDA(expr)                                                   \
+  do {                                                                \
+    cudaError_t _e = (expr);                                          \
+    if (_e != cudaSuccess) { cleanup(); return cuda_fail(c, _e, #expr); } \
+  } while (0)
+  BTRY(dalloc(c, &B.bx, B.nn));
+  BTRY(dalloc(c, &B.xx, B.nn));
+  BTRY(dalloc(c, &B.rx, B.nn));
+  BTRY(dalloc(c, &B.px, B.nn));
+  BTRY(dalloc(c, &B.qx, B.nn));
+  BTRY(dalloc(c, &B.s, 1));
+  BTRY(dalloc(c, &B.partials, (int64_t)std::max(B.g_spmv, B.g_vec) * kNvMax * kMaxRhs));
+  BTRY(dalloc(c, &restart_dev, kMaxRhs));
+  BCUDA(cudaMallocHost((void**)&hs, sizeof(BScalars)));
+  cudaEvent_t t0, t1;
+  BCUDA(cudaEventCreate(&t0));
+  BCUDA(cudaEventCreate(&t1));
+  BCUDA(cudaEventRecord(t0, c->stream));
+  c->launches = 0;
+
+  const int gi = grid_blocks(B.nn);
+  k_interleave<<<gi, kBlk, 0, c->stream>>>(c->n, nrhs, nr, Bm, B.bx);
+  if (algo->use_x0)
+    k_interleave<<<gi, kBlk, 0, c->stream>>>(c->n, nrhs, nr, X, B.xx);
+  else
+    BCUDA(cudaMemsetAsync(B.xx, 0, sizeof(double) * B.nn, c->stream));
+  BScalars h{};
+  h.nr = nr;
+  h.max_iter = algo->max_iter;
+  BCUDA(cudaMemcpyAsync(B.s, &h, sizeof(BScalars), cudaMemcpyHostToDevice, c->stream));
+
+  std::vector<double> tol(nr, 0.0), bnorm(nr, 1.0);
+  std::vector<int> n_refine(nr, 0);
+  switch (G) {
+    case 1: status = pcg_block_run<1>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st); break;
+    case 2: status = pcg_block_run<2>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st); break;
+    case 4: status = pcg_block_run<4>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st); break;
+    default: status = pcg_block_run<8>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st); break;
+  }
+  if (status != UFC_STATUS_OK) {
+    cleanup();
+    return status;
   }
   // final FP64 residual already in hs->true_rr
-  k_deinterleave<<<gv, kBlk, 0, c->stream>>>(c->n, nrhs, nr, xx, X);
+  k_deinterleave<<<gi, kBlk, 0, c->stream>>>(c->n, nrhs, nr, B.xx, X);
   BCUDA(cudaGetLastError());
   BCUDA(cudaEventRecord(t1, c->stream));
   BCUDA(cudaEventSynchronize(t1));
@@ -388,6 +598,8 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* B, double* X, const ufc_solv
   cudaEventElapsedTime(&ms, t0, t1);
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
+  c->timing = ufc_timing_info{};
+  c->timing.kernel_launches = c->launches + 2;
   bool all = true;
   for (int k = 0; k < nrhs; ++k) {
     ufc_solver_state& sk = st[k];

@@ -612,8 +612,12 @@ int ufc_nr_increment(ufc_ctx* c, ufc_nr_arg* a) {
   }
   ufc_solver_algo lin = a->lin;
   lin.use_x0 = 0;
-  const int build = UFC_BUILD_FP64;  // the tangent is not the linear-elastic operator: FP64 CG
-  lin.precision_mode = UFC_PRECISION_FP64;
+  // FP64 CG on the FP64 tangent, or (UFC_PRECISION_FP32_REFINE) FP32 CG on the
+  // tangent rounded from its FP64 assembly, whose FP64 values give the
+  // refinement residual
+  if (lin.precision_mode != UFC_PRECISION_FP32_REFINE) lin.precision_mode = UFC_PRECISION_FP64;
+  const int build =
+      lin.precision_mode == UFC_PRECISION_FP64 ? UFC_BUILD_FP64 : (UFC_BUILD_FP64 | UFC_BUILD_FP32_ROUNDED);
   const int vg = std::min(grid_for(c->n, 256), 148 * 8);
   for (int it = 0; it < a->max_iterations; ++it) {
     UFC_TRY(compute_fint(c, c->u, c->nr_fint, true));

@@ -46,26 +46,32 @@ int vec_grid(int64_t n) {
 
 enum SpmvMode { kPlain = 0, kCg = 1 };
 
-// y = K x, one thread per block row of a SELL-32 slice (a warp = a slice).
+// y = K x over SELL-32 slices: one thread per block row, SPLIT warps per slice.
+// With SPLIT > 1 the warps of a slice take the stored blocks j = part,
+// part + SPLIT, ... of their 32 rows (every load stays a coalesced 32-row
+// line) and their partial row sums are added in shared memory in warp order,
+// so the result depends only on SPLIT, which the launcher derives from the
+// problem size (more warps in flight for meshes with few slices per SM).
 // TV: stored value type, TX: vector type, TA: accumulator type of the row sums.
 // DIFF: values in difference form (diagonal slot = block row sum S_i), so the
 // row is evaluated as sum_{j != i} K_ij (x_j - x_i) + S_i x_i.
-template <typename TV, typename TX, typename TA, int MODE, bool DIFF>
+template <typename TV, typename TX, typename TA, int MODE, bool DIFF, int SPLIT>
 __global__ void __launch_bounds__(kSpmvBlock)
-    k_spmv(int32_t N, int64_t nrows_pad, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
+    k_spmv(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
            const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y, CgScalars* __restrict__ scal,
            double* __restrict__ partials) {
   if (MODE == kCg && scal->stop) return;
-  const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
-  double dot[1] = {0.0};
-  if (row < nrows_pad) {
-    const int64_t s = row >> 5;
-    const int t = (int)(row & 31);
+  constexpr int kWarps = kSpmvBlock / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int part = warp % SPLIT;
+  const int64_t s = (int64_t)blockIdx.x * (kWarps / SPLIT) + warp / SPLIT;
+  const int64_t row = s * kSlice + lane;
+  TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
+  if (s < nslices) {
     const int64_t base = sptr[s];
     const int len = (int)((sptr[s + 1] - base) >> 5);
-    const int32_t* cp = col + base + t;
-    const TV* vp = val + 9 * base + t;
-    TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
+    const int32_t* cp = col + base + lane;
+    const TV* vp = val + 9 * base + lane;
     TA xi0 = TA(0), xi1 = TA(0), xi2 = TA(0);
     if (DIFF && row < N) {
       xi0 = (TA)x[3 * row];
@@ -73,7 +79,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
       xi2 = (TA)x[3 * row + 2];
     }
 #pragma unroll 2
-    for (int j = 0; j < len; ++j) {
+    for (int j = part; j < len; j += SPLIT) {
       const int64_t cj = __ldcs(cp + 32 * j);
       TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
       if (DIFF && cj != row) {
@@ -86,13 +92,28 @@ __global__ void __launch_bounds__(kSpmvBlock)
       a1 += (TA)__ldcs(v + 96) * x0 + (TA)__ldcs(v + 128) * x1 + (TA)__ldcs(v + 160) * x2;
       a2 += (TA)__ldcs(v + 192) * x0 + (TA)__ldcs(v + 224) * x1 + (TA)__ldcs(v + 256) * x2;
     }
-    if (row < N) {
-      y[3 * row] = (TX)a0;
-      y[3 * row + 1] = (TX)a1;
-      y[3 * row + 2] = (TX)a2;
-      if (MODE == kCg)
-        dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
+  }
+  if constexpr (SPLIT > 1) {
+    __shared__ TA sh[kWarps][3][32];
+    sh[warp][0][lane] = a0;
+    sh[warp][1][lane] = a1;
+    sh[warp][2][lane] = a2;
+    __syncthreads();
+    if (part == 0) {
+#pragma unroll
+      for (int q = 1; q < SPLIT; ++q) {
+        a0 += sh[warp + q][0][lane];
+        a1 += sh[warp + q][1][lane];
+        a2 += sh[warp + q][2][lane];
+      }
     }
+  }
+  double dot[1] = {0.0};
+  if (part == 0 && s < nslices && row < N) {
+    y[3 * row] = (TX)a0;
+    y[3 * row + 1] = (TX)a1;
+    y[3 * row + 2] = (TX)a2;
+    if (MODE == kCg) dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
   }
   if (MODE == kCg) {
     double tot[1];
@@ -105,6 +126,51 @@ __global__ void __launch_bounds__(kSpmvBlock)
       }
     }
   }
+}
+
+// Warps per SELL slice: the smallest power of two (<= 8) that puts at least
+// 32 warps per SM in flight.
+int spmv_split(const Ctx* c) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  int split = 1;
+  while (split < 8 && c->nslices * split < (int64_t)sms * 32) split <<= 1;
+  return split;
+}
+
+template <typename TV, typename TX, typename TA, int MODE, bool DIFF, int SPLIT>
+void launch_spmv_split(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
+  constexpr int per_block = kSpmvBlock / 32 / SPLIT;
+  const int grid = (int)((c->nslices + per_block - 1) / per_block);
+  k_spmv<TV, TX, TA, MODE, DIFF, SPLIT><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices, c->slice_ptr, c->sell_col,
+                                                                      val, x, y, c->scal, c->partials);
+}
+
+template <typename TV, typename TX, typename TA, int MODE, bool DIFF>
+void launch_spmv_diff(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
+  switch (spmv_split(c)) {
+    case 1: launch_spmv_split<TV, TX, TA, MODE, DIFF, 1>(c, st, val, x, y); break;
+    case 2: launch_spmv_split<TV, TX, TA, MODE, DIFF, 2>(c, st, val, x, y); break;
+    case 4: launch_spmv_split<TV, TX, TA, MODE, DIFF, 4>(c, st, val, x, y); break;
+    default: launch_spmv_split<TV, TX, TA, MODE, DIFF, 8>(c, st, val, x, y); break;
+  }
+}
+
+// SELL SpMV over the full (non-symmetric) storage; the FP32 difference form
+// when the FP32 values were built that way.
+template <typename TV, typename TX, typename TA, int MODE>
+void launch_spmv(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
+  if constexpr (sizeof(TV) == 4) {
+    if (c->val32_diff) {
+      launch_spmv_diff<TV, TX, TA, MODE, true>(c, st, val, x, y);
+      return;
+    }
+  }
+  launch_spmv_diff<TV, TX, TA, MODE, false>(c, st, val, x, y);
 }
 
 // y = K x from the symmetric storage: row i sums its upper blocks K_ij x_j
@@ -390,12 +456,8 @@ void launch_iteration(const Run& R, const Vecs<TV, TX>& V, cudaStream_t st, cuda
   if (ev0) cudaEventRecord(ev0, st);
   if (V.sym)
     launch_spmv_sym<TV, TX, TA, kCg>(c, R.sg, st, V.val, V.p, V.q);
-  else if (sizeof(TV) == 4 && c->val32_diff)
-    k_spmv<TV, TX, TA, kCg, true><<<R.sg, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col,
-                                                               V.val, V.p, V.q, c->scal, c->partials);
   else
-    k_spmv<TV, TX, TA, kCg, false><<<R.sg, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col,
-                                                                V.val, V.p, V.q, c->scal, c->partials);
+    launch_spmv<TV, TX, TA, kCg>(c, st, V.val, V.p, V.q);
   if (ev1) cudaEventRecord(ev1, st);
   k_cg_update<TX><<<R.vg, kVecBlock, 0, st>>>(R.n, V.p, V.q, V.r, c->x64, V.dinv, c->scal, c->partials);
   k_cg_pupdate<TX><<<R.vg, kVecBlock, 0, st>>>(R.n, V.r, V.dinv, V.p, c->scal);
@@ -403,14 +465,16 @@ void launch_iteration(const Run& R, const Vecs<TV, TX>& V, cudaStream_t st, cuda
 }
 
 // FP64 residual of the current x64 into y64 / r-source, true_rr on the device.
+// FP64 runs use their own matrix; refined FP32 runs use the matrix-free FP64
+// element operator for the linear-elastic material and the assembled FP64
+// values otherwise (the J2 tangent).
 int true_residual(const Run& R, bool want_bb) {
   Ctx* c = R.c;
-  if (R.prec == UFC_PRECISION_FP64) {
+  if (R.prec == UFC_PRECISION_FP64 || c->mat_model != UFC_MAT_ELASTIC_ISO) {
     if (c->has_sval64)
       launch_spmv_sym<double, double, double, kPlain>(c, R.sg, c->stream, c->sval64, c->x64, c->y64);
     else
-      k_spmv<double, double, double, kPlain, false><<<R.sg, kSpmvBlock, 0, c->stream>>>(
-          c->N, c->nslices * kSlice, c->slice_ptr, c->sell_col, c->val64, c->x64, c->y64, nullptr, nullptr);
+      launch_spmv<double, double, double, kPlain>(c, c->stream, c->val64, c->x64, c->y64);
     UFC_CUDA(c, cudaGetLastError());
     c->launches += 1;
   } else {
@@ -719,34 +783,24 @@ int64_t spmv_bytes(const Ctx* c, int precision) {
 int spmv(Ctx* c, int precision, const void* x, void* y) {
   if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: pattern not built");
   const int sg = (int)((c->nslices * kSlice + kSpmvBlock - 1) / kSpmvBlock);
-  const int64_t np = c->nslices * kSlice;
   if (precision == UFC_PRECISION_FP64) {
     if (!c->has_val64) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP64 values not assembled");
     if (c->has_sval64)
       launch_spmv_sym<double, double, double, kPlain>(c, sg, c->stream, c->sval64, (const double*)x, (double*)y);
     else
-      k_spmv<double, double, double, kPlain, false><<<sg, kSpmvBlock, 0, c->stream>>>(
-          c->N, np, c->slice_ptr, c->sell_col, c->val64, (const double*)x, (double*)y, nullptr, nullptr);
+      launch_spmv<double, double, double, kPlain>(c, c->stream, c->val64, (const double*)x, (double*)y);
   } else if (precision == UFC_PRECISION_FP32_REFINE) {
     if (!c->has_val32) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP32 values not assembled");
     if (c->has_sval32)
       launch_spmv_sym<float, float, float, kPlain>(c, sg, c->stream, c->sval32, (const float*)x, (float*)y);
-    else if (c->val32_diff)
-      k_spmv<float, float, float, kPlain, true><<<sg, kSpmvBlock, 0, c->stream>>>(
-          c->N, np, c->slice_ptr, c->sell_col, c->val32, (const float*)x, (float*)y, nullptr, nullptr);
     else
-      k_spmv<float, float, float, kPlain, false><<<sg, kSpmvBlock, 0, c->stream>>>(
-          c->N, np, c->slice_ptr, c->sell_col, c->val32, (const float*)x, (float*)y, nullptr, nullptr);
+      launch_spmv<float, float, float, kPlain>(c, c->stream, c->val32, (const float*)x, (float*)y);
   } else if (precision == UFC_PRECISION_FP32_MATRIX) {
     if (!c->has_val32) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: FP32 values not assembled");
     if (c->has_sval32)
       launch_spmv_sym<float, double, double, kPlain>(c, sg, c->stream, c->sval32, (const double*)x, (double*)y);
-    else if (c->val32_diff)
-      k_spmv<float, double, double, kPlain, true><<<sg, kSpmvBlock, 0, c->stream>>>(
-          c->N, np, c->slice_ptr, c->sell_col, c->val32, (const double*)x, (double*)y, nullptr, nullptr);
     else
-      k_spmv<float, double, double, kPlain, false><<<sg, kSpmvBlock, 0, c->stream>>>(
-          c->N, np, c->slice_ptr, c->sell_col, c->val32, (const double*)x, (double*)y, nullptr, nullptr);
+      launch_spmv<float, double, double, kPlain>(c, c->stream, c->val32, (const double*)x, (double*)y);
   } else {
     return fail(c, UFC_STATUS_INVALID, "ufc_spmv: precision");
   }
@@ -766,9 +820,10 @@ int pcg_solve(Ctx* c, const double* b, double* x, const ufc_solver_algo* algo, u
     return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: precision_mode");
   if (prec != UFC_PRECISION_FP64 && !c->has_val32)
     return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: FP32 values not assembled (UFC_BUILD_FP32*)");
-  if (prec != UFC_PRECISION_FP64 && c->mat_model != UFC_MAT_ELASTIC_ISO)
-    return fail(c, UFC_STATUS_UNSUPPORTED,
-                "ufc_pcg_solve: FP32 matrices need the linear-elastic FP64 element operator for their residual");
+  if (prec != UFC_PRECISION_FP64 && c->mat_model != UFC_MAT_ELASTIC_ISO && !c->has_val64)
+    return fail(c, UFC_STATUS_INVALID,
+                "ufc_pcg_solve: refined FP32 solves of a non-elastic tangent need its FP64 values for the residual "
+                "(UFC_BUILD_FP64 | UFC_BUILD_FP32_ROUNDED)");
   if (prec == UFC_PRECISION_FP32_MATRIX && algo->precond_type == UFC_SOLV_PREC_JACOBI && !c->has_val64)
     return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: FP32_MATRIX takes its Jacobi diagonal from the FP64 values");
   UFC_TRY(ensure_vectors(c, prec));
