@@ -242,6 +242,69 @@ typedef struct {
   int32_t status;             /* [OUT] */
 } ufc_nr_arg;
 
+/* One analysis step with automatic increments: RT_StepDriver_Execute
+ * (ufc_core/L5_RT/StepDriver/RT_Step_Exec.f90:415-600) with the increment
+ * control of RT_StepDriver_End_Increment / RT_StepDriver_Cutback
+ * (RT_Step_Core.f90:215-300, defaults RT_Step_Def.f90:147-153).  The prescribed
+ * values and the external force are ramped linearly in step time from their
+ * values at the start of the step (the committed displacement, f_ext_start) to
+ * u_prescribed_end / f_ext_end at time_period.  Each increment runs
+ * ufc_nr_increment; a converged increment is committed, and the next one grows
+ * by growth_factor when it took <= (int)(target_iters * growth_threshold)
+ * Newton iterations (capped by dt_max and the end of the step); a failed one is
+ * rolled back and retried with dt * cutback_factor, the step failing when dt
+ * drops below dt_min or more than max_cutbacks cutbacks follow one another. */
+typedef struct {
+  const double* u_prescribed_end; /* [IN] [n_fixed] Dirichlet values at the end of the step, or NULL (kept) */
+  const double* f_ext_start;      /* [IN] [n_dof] external force at the start of the step, or NULL (zero) */
+  const double* f_ext_end;        /* [IN] [n_dof] external force at the end of the step, or NULL (zero) */
+  int32_t mem;                    /* [IN] memory of the three arrays */
+  double time_period;             /* [IN] step time, > 0 */
+  double dt_initial, dt_min, dt_max; /* [IN] increment sizes in step time */
+  int32_t max_increments;         /* [IN] attempted increments, converged or not */
+  int32_t max_cutbacks;           /* [IN] consecutive cutbacks before the step fails */
+  int32_t auto_dt;                /* [IN] 1: grow dt after easy increments (RT_Step_Stp_Ctl_Algo%auto_dt) */
+  int32_t target_iters;           /* [IN] 6 in the reference */
+  double growth_threshold;        /* [IN] 0.8 */
+  double growth_factor;           /* [IN] 1.25 */
+  double cutback_factor;          /* [IN] 0.5 */
+  int32_t max_iterations;         /* [IN] Newton iterations per increment */
+  double tolerance_force;         /* [IN] as ufc_nr_arg */
+  ufc_solver_algo lin;            /* [IN] linear solver of every Newton iteration */
+  double* hist_time;              /* [OUT] host [hist_cap]: step time at the end of each attempt, or NULL */
+  double* hist_dt;                /* [OUT] host [hist_cap]: increment size of each attempt, or NULL */
+  int32_t* hist_iters;            /* [OUT] host [hist_cap]: Newton iterations of each attempt, or NULL */
+  int32_t* hist_converged;        /* [OUT] host [hist_cap]: 1 converged, 0 cut back, or NULL */
+  int32_t hist_cap;               /* [IN] */
+  int32_t attempts;               /* [OUT] increments attempted (entries written: min(attempts, hist_cap)) */
+  int32_t increments;             /* [OUT] converged increments */
+  int32_t cutbacks;               /* [OUT] total cutbacks */
+  int32_t nr_iterations;          /* [OUT] Newton iterations of the converged increments */
+  int64_t lin_iters_total;        /* [OUT] CG iterations of all attempts */
+  double final_time;              /* [OUT] step time reached */
+  int32_t completed;              /* [OUT] 1 when final_time reached time_period */
+  int32_t status;                 /* [OUT] */
+} ufc_step_arg;
+
+/* Equivalent nodal forces of face loads on C3D8 faces: the 2x2 face Gauss rule
+ * of PH_Elem_C3D8_FormFacePressure (ufc_core/L4_PH/Element/Solid3D/PH_Elem_C3D8.f90:2360-2541)
+ * and its face numbering (1: nodes 1-2-3-4, zeta = -1; 2: 5-8-7-6, zeta = +1;
+ * 3: 1-2-6-5, eta = -1; 4: 4-3-7-8, eta = +1; 5: 1-4-8-5, xi = -1; 6: 2-6-7-3,
+ * xi = +1), with N_a = (1/8)(1 +- xi)(1 +- eta)(1 +- zeta).  Per face, a
+ * traction vector t (force per unit area) and/or a pressure p acting against
+ * the outward normal: f_a += sum_gp N_a (t - p n_out) dA.  Faces are assembled
+ * in element-colour order, so the result is deterministic; f is overwritten. */
+typedef struct {
+  int32_t n_faces;         /* [IN] */
+  const int32_t* elem;     /* [IN] [n_faces] element ids (index_base) */
+  const int32_t* face;     /* [IN] [n_faces] face ids 1..6 */
+  const double* traction;  /* [IN] [n_faces][3] or NULL */
+  const double* pressure;  /* [IN] [n_faces] or NULL */
+  int32_t index_base;      /* [IN] 0 or 1 */
+  int32_t mem;             /* [IN] memory of every array */
+  double* f;               /* [OUT] [n_dof] */
+} ufc_face_load_arg;
+
 /* Device-time counters of the last ufc_pcg_solve (filled when instrumentation
  * is on, see ufc_ctx_set_instrument). */
 typedef struct {
@@ -283,6 +346,24 @@ int ufc_mat_update_batch(ufc_ctx* ctx, ufc_mat_update_arg* arg);
  * committed state and ignore u.  Either output may be NULL. */
 int ufc_stress_eval(ufc_ctx* ctx, const double* u, double* stress_gp, double* vm_gp, int32_t mem);
 
+/* ---- loads and output on either side of the solve ---- */
+/* External load vector from face tractions / pressures (RT_Asm_GlobalLoad's
+ * surface-load branch, ufc_core/L5_RT/Assembly/RT_Asm_Solv.f90:1443). */
+int ufc_load_faces(ufc_ctx* ctx, const ufc_face_load_arg* arg);
+/* Nodal stress ([n_nodes][6]) and von Mises of that stress ([n_nodes]): the
+ * Gauss-point stress of each element extrapolated to its nodes with the
+ * inverse of the Gauss-point interpolation matrix (PH_Elem_C3D8_GetExtrapMat /
+ * PH_Elem_C3D8_MapToNode, PH_Elem_C3D8.f90:2782-2824, with N_a = (1/8)...),
+ * then averaged over the elements that share the node (colour-ordered,
+ * deterministic).  u as ufc_stress_eval; either output may be NULL. */
+int ufc_stress_nodal(ufc_ctx* ctx, const double* u, double* stress_node, double* vm_node, int32_t mem);
+/* Reaction forces RF = F_int(u) - F_ext at the prescribed DOFs, in the order of
+ * ufc_bc_desc (the constrained rows of R = F_ext - F_int of
+ * RT_Asm_ComputeResidual, RT_Asm_Solv.f90:1311-1426).  u NULL: the current
+ * displacement; f_ext NULL: zero.  J2 models use the trial state of u without
+ * changing it. */
+int ufc_reactions(ufc_ctx* ctx, const double* u, const double* f_ext, double* rf, int32_t mem);
+
 /* ---- linear algebra ---- */
 /* y = K x with the assembled matrix of the given precision (RT_CSRMatrix_matvec,
  * ufc_core/L2_NM/Matrix/NM_Assem_Sparse.f90:199-212).  UFC_PRECISION_FP32_REFINE
@@ -307,6 +388,9 @@ int ufc_last_residual_history(ufc_ctx* ctx, double* out, int32_t max_len, int32_
 
 /* ---- nonlinear driver and material state (RT_Step_Exec.f90:415-600) ---- */
 int ufc_nr_increment(ufc_ctx* ctx, ufc_nr_arg* arg);
+/* Returns UFC_STATUS_OK when the step completed, UFC_STATUS_NOT_CONVERGED when
+ * it failed (the state is that of the last converged increment). */
+int ufc_nr_step(ufc_ctx* ctx, ufc_step_arg* arg);
 int ufc_state_commit(ufc_ctx* ctx);
 int ufc_state_rollback(ufc_ctx* ctx);
 /* Current displacement held by the context ([n_dof]). */

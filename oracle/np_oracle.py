@@ -89,3 +89,81 @@ def j2_tensor(props, deps_voigt, sig_n_voigt, epeq_n):
     dg = f / (3 * G + H)
     S = (1 - 3 * G * dg / q) * dev + p * np.eye(3)
     return tensor_to_voigt_stress(S), epeq_n + dg
+
+
+# ---------------------------------------------------------------- loads and output
+# Face numbering and 2x2 face rule of PH_Elem_C3D8_FormFacePressure
+# (ufc_core/L4_PH/Element/Solid3D/PH_Elem_C3D8.f90:2360-2541): face id ->
+# (fixed parametric direction, its value, in-plane directions u and v, face nodes).
+FACES = {1: (2, -1.0, 0, 1, (0, 1, 2, 3)), 2: (2, 1.0, 0, 1, (4, 7, 6, 5)),
+         3: (1, -1.0, 0, 2, (0, 1, 5, 4)), 4: (1, 1.0, 0, 2, (3, 2, 6, 7)),
+         5: (0, -1.0, 1, 2, (0, 3, 7, 4)), 6: (0, 1.0, 1, 2, (1, 5, 6, 2))}
+
+
+def shape_n(xi):
+    """N [8] at one parametric point (ComputeShape_Hex8, factor 1/8)."""
+    return 0.125 * np.prod(1.0 + SIGNS * np.asarray(xi)[None, :], axis=1)
+
+
+def face_load(X, face_id, traction=None, pressure=0.0):
+    """Nodal forces [8,3] of one face: sum over the 2x2 face points of
+    N_a (t - p n_out) dA, n_out the outward unit normal, found here from the
+    element centroid (independent of the kernels' orientation table)."""
+    fixed, val, ud, vd, nodes = FACES[face_id]
+    t = np.zeros(3) if traction is None else np.asarray(traction, dtype=np.float64)
+    F = np.zeros((8, 3))
+    centroid = X.mean(axis=0)
+    for gu in (-G1, G1):
+        for gv in (-G1, G1):
+            xi = np.zeros(3)
+            xi[fixed], xi[ud], xi[vd] = val, gu, gv
+            N = shape_n(xi)
+            dN = shape_grad(xi)
+            du, dv = dN[:, ud] @ X, dN[:, vd] @ X
+            n = np.cross(du, dv)
+            dA = np.linalg.norm(n)
+            if dA < 1e-15:
+                continue
+            n /= dA
+            if np.dot(n, N @ X - centroid) < 0:  # make it point away from the element
+                n = -n
+            F += np.outer(N, t - pressure * n) * dA
+    for a in range(8):
+        if a not in nodes:
+            assert np.allclose(F[a], 0.0)
+    return F
+
+
+def face_loads(coords, conn, elem, face, traction=None, pressure=None):
+    f = np.zeros(3 * coords.shape[0])
+    for k in range(len(elem)):
+        e = int(elem[k])
+        X = coords[conn[e]]
+        Fe = face_load(X, int(face[k]), None if traction is None else traction[k],
+                       0.0 if pressure is None else pressure[k])
+        for a in range(8):
+            f[3 * conn[e, a]:3 * conn[e, a] + 3] += Fe[a]
+    return f
+
+
+def extrap_matrix():
+    """(A^T)^-1 with A[a, ip] = N_a(Gauss point ip): nodal values from the
+    eight Gauss-point values (PH_Elem_C3D8_GetExtrapMat, PH_Elem_C3D8.f90:2782-2800),
+    Gauss points in the xi-fastest order of GAUSS."""
+    A = np.stack([shape_n(g) for g in GAUSS], axis=1)  # [8 nodes, 8 points]
+    return np.linalg.inv(A.T)
+
+
+def nodal_stress(n_nodes, conn, sig_gp):
+    """Extrapolate [E,8,6] Gauss-point stress to the element nodes and average
+    over the elements sharing each node; returns ([N,6], von Mises [N])."""
+    Ex = extrap_matrix()
+    per_node = np.einsum("ai,eic->eac", Ex, sig_gp)
+    s = np.zeros((n_nodes, 6))
+    cnt = np.zeros(n_nodes)
+    np.add.at(s, conn.ravel(), per_node.reshape(-1, 6))
+    np.add.at(cnt, conn.ravel(), 1.0)
+    s /= np.maximum(cnt, 1.0)[:, None]
+    p = s[:, :3].mean(axis=1)
+    j2 = 0.5 * ((s[:, :3] - p[:, None]) ** 2).sum(axis=1) + (s[:, 3:] ** 2).sum(axis=1)
+    return s, np.sqrt(3.0 * np.maximum(j2, 0.0))

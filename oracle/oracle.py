@@ -257,55 +257,118 @@ def pcg(K: CSR, b, x0=None, rtol=1e-10, atol=0.0, max_iter=100000):
     return x, {"status": st, "iters": it.value, "res_final": rf.value, "res_init": ri.value}
 
 
-def nr_j2(model: Model, targets, tol=1e-8, max_iter=25, lin_rtol=1e-10):
-    """Displacement-controlled J2 Newton-Raphson over the increments whose
-    prescribed DOF values are ``targets`` (list of arrays).  Each iteration
+def nr_increment_j2(model: Model, u, state, tgt, tol=1e-8, max_iter=25, lin_rtol=1e-10):
+    """One displacement-controlled J2 Newton-Raphson increment from the
+    committed (u, state) to the prescribed values ``tgt``
+    (RT_NLSolver_NewtonRaph, RT_Solv_Nonlin.f90:807-1002).  Each iteration
     updates every Gauss point from the committed state, assembles the
     consistent tangent and internal force, and solves K du = -R_free with
-    Jacobi-PCG (RT_NLSolver_NewtonRaph, RT_Solv_Nonlin.f90:807-1002).
-    Convergence: ||R_free|| <= tol * max(||F_int||, 1e-30), F_int over every
-    DOF (the reaction scale; the reference divides by ||F_ext||,
-    RT_Step_NR_Core.f90:252-258, which is zero under displacement control).
-    The first iteration of an increment is the predictor
-    K_ff du_f = R_f - K_fc du_c (tangent at the start of the increment), after
-    which the prescribed DOFs take their new values.
-    Returns the displacement history, the committed state and per-increment logs."""
+    Jacobi-PCG.  Convergence: ||R_free|| <= tol * max(||F_int||, 1e-30), F_int
+    over every DOF (the reaction scale; the reference divides by ||F_ext||,
+    RT_Step_NR_Core.f90:252-258, which is zero under displacement control),
+    tested before each solve.  The first iteration of an increment is the
+    predictor K_ff du_f = R_f - K_fc du_c (tangent at the start of the
+    increment), after which the prescribed DOFs take their new values.
+    Returns (converged, iterations, u, trial state, log); a non-finite residual
+    or a failed linear solve is a non-convergence."""
     p = model.p
+    u = u.copy()
+    u_n = u.copy()
+    free = np.ones(model.n, dtype=bool)
+    free[p.fixed] = False
+    dc = np.zeros(model.n)
+    dc[p.fixed] = tgt - u[p.fixed]
+    lift = bool(np.any(dc != 0.0))
+    log = []
+    trial = None
+    for it in range(max_iter):
+        fint, trial = model.fint_j2(u, u_n, state)
+        R = -fint
+        R[~free] = 0.0
+        rn = np.linalg.norm(R)
+        fn = max(np.linalg.norm(fint), 1e-30)
+        log.append(rn / fn)
+        if not np.isfinite(rn):
+            return False, it, u, trial, log
+        if not lift and rn <= tol * fn:
+            return True, it, u, trial, log
+        K = model.assemble(Dgp=trial["D"])
+        if lift:
+            y = model.assemble(Dgp=trial["D"], eliminate=False).matvec(dc)
+            R[free] -= y[free]
+        du, info = pcg(K, R, rtol=lin_rtol)
+        if info["status"] != 0:
+            return False, it, u, trial, log
+        u += du
+        if lift:
+            u[p.fixed] = tgt
+            lift = False
+    return False, max_iter, u, trial, log
+
+
+def nr_j2(model: Model, targets, tol=1e-8, max_iter=25, lin_rtol=1e-10):
+    """Increments whose prescribed DOF values are ``targets`` (list of arrays),
+    each solved by nr_increment_j2 from the previous converged one.  Returns
+    the displacement history, the committed state and per-increment logs."""
     G = model.E * 8
     state = {"sig": np.zeros(G * 6), "epeq": np.zeros(G), "epl": np.zeros(G * 6)}
     u = np.zeros(model.n)
-    free = np.ones(model.n, dtype=bool)
-    free[p.fixed] = False
     hist, logs = [], []
     for tgt in targets:
-        u_n = u.copy()
-        dc = np.zeros(model.n)
-        dc[p.fixed] = tgt - u[p.fixed]
-        lift = bool(np.any(dc != 0.0))
-        log = []
-        conv = False
-        for it in range(max_iter):
-            fint, trial = model.fint_j2(u, u_n, state)
-            R = -fint
-            R[~free] = 0.0
-            rn = np.linalg.norm(R)
-            fn = max(np.linalg.norm(fint), 1e-30)
-            log.append(rn / fn)
-            if not lift and rn <= tol * fn:
-                conv = True
-                break
-            K = model.assemble(Dgp=trial["D"])
-            if lift:
-                y = model.assemble(Dgp=trial["D"], eliminate=False).matvec(dc)
-                R[free] -= y[free]
-            du, info = pcg(K, R, rtol=lin_rtol)
-            u += du
-            if lift:
-                u[p.fixed] = tgt
-                lift = False
+        conv, _, u, trial, log = nr_increment_j2(model, u, state, tgt, tol, max_iter, lin_rtol)
         if not conv:
             raise RuntimeError("NR did not converge")
         state = {"sig": trial["sig"], "epeq": trial["epeq"], "epl": trial["epl"]}
         hist.append(u.copy())
         logs.append(log)
     return hist, state, logs
+
+
+def step_j2(model: Model, u_end, time_period=1.0, dt_initial=1.0, dt_min=1e-5, dt_max=1.0, max_increments=100,
+            max_cutbacks=5, auto_dt=True, target_iters=6, growth_threshold=0.8, growth_factor=1.25,
+            cutback_factor=0.5, tol=1e-8, max_iter=25, lin_rtol=1e-10):
+    """One step with automatic increments, from zero displacement and state to
+    the prescribed values ``u_end`` ramped linearly in step time: the increment
+    loop of RT_StepDriver_Execute (ufc_core/L5_RT/StepDriver/RT_Step_Exec.f90:415-600)
+    with RT_StepDriver_End_Increment / RT_StepDriver_Cutback
+    (RT_Step_Core.f90:215-300): after a converged increment dt grows by
+    growth_factor when it took <= int(target_iters * growth_threshold) Newton
+    iterations (capped by dt_max); a failed one is discarded and retried with
+    dt * cutback_factor, the step failing below dt_min or after more than
+    max_cutbacks consecutive cutbacks.  Returns a dict with the attempt history
+    rows (time, dt, iterations, converged)."""
+    p = model.p
+    G = model.E * 8
+    state = {"sig": np.zeros(G * 6), "epeq": np.zeros(G), "epl": np.zeros(G * 6)}
+    u = np.zeros(model.n)
+    u0 = u[p.fixed].copy()
+    u_end = np.asarray(u_end, dtype=np.float64)
+    T = float(time_period)
+    t, dt = 0.0, min(dt_initial, dt_max)
+    cut_run, attempts, increments, cutbacks, hist = 0, 0, 0, 0, []
+    while t < T * (1.0 - 1e-12) and attempts < max_increments:
+        dt = min(dt, T - t)
+        t1 = t + dt
+        s = 1.0 if t1 >= T else t1 / T
+        tgt = u0 + s * (u_end - u0)
+        conv, it, u_new, trial, _ = nr_increment_j2(model, u, state, tgt, tol, max_iter, lin_rtol)
+        attempts += 1
+        hist.append((t1, dt, it, conv))
+        if conv:
+            u = u_new
+            state = {"sig": trial["sig"], "epeq": trial["epeq"], "epl": trial["epl"]}
+            t = T if t1 >= T else t1
+            increments += 1
+            cut_run = 0
+            if auto_dt and it <= int(target_iters * growth_threshold):
+                dt = min(dt * growth_factor, dt_max)
+            continue
+        cutbacks += 1
+        cut_run += 1
+        if cut_run > max_cutbacks:
+            break
+        dt *= cutback_factor
+        if dt < dt_min:
+            break
+    return {"completed": t >= T * (1.0 - 1e-12), "final_time": t, "history": hist, "u": u, "state": state,
+            "increments": increments, "cutbacks": cutbacks, "attempts": attempts}

@@ -112,3 +112,82 @@ def test_j2_bar_64x32x32_uniaxial(pkg):
     area = p.shape[1] * p.shape[2]
     assert abs(fint[pull].sum() - sigma * area) <= 1e-6 * sigma * area
     assert total_iters <= 20 * 6
+
+
+def _step_kw(**kw):
+    base = dict(dt_min=1e-3, max_cutbacks=6, growth_factor=1.25, cutback_factor=0.5, target_iters=6,
+                growth_threshold=0.8)
+    base.update(kw)
+    return base
+
+
+def _compare_history(res, ref, iters_slack=0):
+    assert len(res.history) == len(ref["history"])
+    for (t, dt, it, ok), (t_o, dt_o, it_o, ok_o) in zip(res.history, ref["history"]):
+        assert ok == ok_o and abs(it - it_o) <= iters_slack, ((t, dt, it, ok), (t_o, dt_o, it_o, ok_o))
+        assert t == t_o and dt == dt_o  # the same IEEE operations on the same decisions
+
+
+@pytest.mark.parametrize("max_iter,dt0,max_inc", [(2, 1.0, 60)])
+def test_step_driver_history_matches_oracle(pkg, orc, max_iter, dt0, max_inc):
+    """RT_StepDriver increment control: cutbacks after non-converged increments,
+    growth after easy ones; the attempt history (time, dt, Newton iterations,
+    converged) equals the oracle's.  With two Newton iterations an increment
+    converges exactly when it stays elastic (one predictor solve) and fails when
+    it crosses the yield point, so every decision is clear of the force
+    tolerance; the histories must agree entry for entry."""
+    p = pkg.mesh.j2_bar(4, 2, 2)
+    u_end = pkg.mesh.j2_bar_target(p, 1, n_steps=1, strain=0.0107)
+    kw = _step_kw(dt_initial=dt0, max_increments=max_inc)
+    ref = orc.step_j2(orc.Model(p), u_end, max_iter=max_iter, lin_rtol=1e-12, **kw)
+    m = _bar_model(pkg, p)
+    res = m.nr_step(u_end, max_iterations=max_iter, lin=pkg.SolverAlgo(tolerance=1e-12), **kw)
+    assert res.cutbacks == ref["cutbacks"] >= 3
+    assert res.increments == ref["increments"] and res.attempts == ref["attempts"]
+    assert not res.completed and res.status == pkg.STATUS_NOT_CONVERGED
+    _compare_history(res, ref)
+    # the context holds the last converged increment
+    np.testing.assert_allclose(m.displacement(), ref["u"], rtol=0, atol=1e-8 * np.abs(ref["u"]).max())
+    assert res.final_time == ref["final_time"]
+
+
+def test_step_driver_completes_to_analytic_state(pkg, orc):
+    p = pkg.mesh.j2_bar(4, 2, 2)
+    strain = 0.01
+    u_end = pkg.mesh.j2_bar_target(p, 1, n_steps=1, strain=strain)
+    kw = _step_kw(dt_initial=0.05, dt_max=0.2, max_increments=80)
+    m = _bar_model(pkg, p)
+    res = m.nr_step(u_end, max_iterations=8, lin=pkg.SolverAlgo(tolerance=1e-12), **kw)
+    ref = orc.step_j2(orc.Model(p), u_end, max_iter=8, lin_rtol=1e-12, **kw)
+    assert res.completed and ref["completed"] and res.final_time == 1.0
+    # plastic increments take 3 Newton iterations, or 4 when the third residual
+    # lands within rounding of the force tolerance; dt grows either way
+    _compare_history(res, ref, iters_slack=1)
+    E, nu, sy, H = PROPS
+    sigma = sy + E * H / (E + H) * (strain - sy / E)
+    _, sig, _ = m.j2_state()
+    np.testing.assert_allclose(sig[..., 0], sigma, rtol=1e-6)
+    # every converged increment was committed: a rollback keeps the end-of-step state
+    m.rollback()
+    np.testing.assert_allclose(m.j2_state()[1][..., 0], sigma, rtol=1e-6)
+
+
+def test_step_driver_elastic_growth(pkg):
+    """Easy increments grow dt by 1.25 up to dt_max; the prescribed values
+    reach their end values exactly."""
+    p = pkg.mesh.j2_bar(3, 2, 2, sy=1e9)
+    u_end = pkg.mesh.j2_bar_target(p, 1, n_steps=1, strain=0.001)
+    m = _bar_model(pkg, p)
+    res = m.nr_step(u_end, dt_initial=0.1, dt_max=0.3, max_increments=20, max_iterations=4,
+                    lin=pkg.SolverAlgo(tolerance=1e-12))
+    assert res.completed and res.cutbacks == 0
+    dts = [h[1] for h in res.history]
+    exp, t, dt = [], 0.0, 0.1
+    while t < 1.0 - 1e-12:
+        dt = min(dt, 1.0 - t)
+        exp.append(dt)
+        t += dt
+        dt = min(dt * 1.25, 0.3)
+    assert dts == exp
+    u = m.displacement()
+    np.testing.assert_array_equal(u[p.fixed], u_end)

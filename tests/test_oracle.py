@@ -198,3 +198,51 @@ def test_nr_j2_homogeneous_bar(pkg, orc):
     epeq = state["epeq"]
     np.testing.assert_allclose(epeq, (eps - sy / E) * E / (E + H), rtol=1e-6)
     assert all(len(lg) <= 6 for lg in logs)
+
+
+def test_face_loads_restatements_agree(pkg):
+    """np_oracle.face_loads (3-D shape functions on the face, normal oriented
+    from the centroid) against mesh.face_traction (bilinear face) on the
+    cantilever end face, and the face-id table against the six box faces."""
+    from oracle import np_oracle as NO
+
+    p = pkg.mesh.config1()
+    nx, ny, nz = p.shape
+    e = pkg.mesh._face_elems(nx, ny, nz, "xmax")
+    f = NO.face_loads(p.coords, p.conn, e, np.full(e.size, 6), np.tile([0.0, 0.0, -1.0], (e.size, 1)))
+    np.testing.assert_allclose(f, p.f, rtol=0, atol=1e-15)
+    X = NO.SIGNS * 0.5 + 0.5  # unit cube
+    want = {1: [0, 0, 1], 2: [0, 0, -1], 3: [0, 1, 0], 4: [0, -1, 0], 5: [1, 0, 0], 6: [-1, 0, 0]}
+    for fid, w in want.items():  # unit pressure pushes into the element
+        np.testing.assert_allclose(NO.face_load(X, fid, pressure=1.0).sum(axis=0), w, atol=1e-15)
+
+
+def test_extrapolation_matrix_closed_form():
+    from oracle import np_oracle as NO
+
+    Ex = NO.extrap_matrix()
+    r3 = np.sqrt(3.0)
+    closed = np.array([[np.prod([(1 + r3 * NO.SIGNS[a, d] * np.sign(NO.GAUSS[ip, d])) / 2 for d in range(3)])
+                        for ip in range(8)] for a in range(8)])
+    np.testing.assert_allclose(Ex, closed, rtol=0, atol=1e-14)
+    np.testing.assert_allclose(Ex.sum(axis=1), 1.0, atol=1e-14)  # constants are reproduced
+    s, vm = NO.nodal_stress(3 * 3 * 3, np.array([[0, 1, 4, 3, 9, 10, 13, 12]]), np.tile([1, 2, 3, 0, 0, 0.5], (1, 8, 1)))
+    np.testing.assert_allclose(s[[0, 1, 4, 3, 9, 10, 13, 12]], np.tile([1, 2, 3, 0, 0, 0.5], (8, 1)), atol=1e-14)
+
+
+def test_oracle_step_driver_growth_sequence(pkg, orc):
+    """Elastic increments converge in one Newton iteration, so dt grows by the
+    growth factor up to dt_max and the last increment is clipped at the end."""
+    p = pkg.mesh.j2_bar(2, 1, 1, sy=1e9)
+    u_end = pkg.mesh.j2_bar_target(p, 1, n_steps=1, strain=0.001)
+    r = orc.step_j2(orc.Model(p), u_end, dt_initial=0.1, dt_max=0.3, max_increments=20)
+    assert r["completed"] and r["cutbacks"] == 0
+    dts = [h[1] for h in r["history"]]
+    exp, t, dt = [], 0.0, 0.1
+    while t < 1.0 - 1e-12:
+        dt = min(dt, 1.0 - t)
+        exp.append(dt)
+        t += dt
+        dt = min(dt * 1.25, 0.3)
+    assert dts == exp and all(h[2] == 1 for h in r["history"])
+    np.testing.assert_array_equal(r["u"][p.fixed], u_end)

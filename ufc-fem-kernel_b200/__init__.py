@@ -13,7 +13,7 @@ include/ufc_gpu.h); this package is its Python host side:
 """
 from . import _abi, mesh  # noqa: F401
 from ._abi import LibraryMissing, check_abi, load  # noqa: F401
-from .fem import FemModel, NrResult, SolverAlgo, SolverState, UfcError, lifted_rhs  # noqa: F401
+from .fem import FemModel, NrResult, SolverAlgo, SolverState, StepResult, UfcError, lifted_rhs  # noqa: F401
 
 PRECISION_FP64 = _abi.PRECISION_FP64
 PRECISION_FP32_REFINE = _abi.PRECISION_FP32_REFINE
@@ -29,3 +29,6 @@ REFINE_KEEP_DIRECTION = _abi.REFINE_KEEP_DIRECTION
 REFINE_RESTART = _abi.REFINE_RESTART
 MAT_ELASTIC_ISO = _abi.MAT_ELASTIC_ISO
 MAT_J2_ISO = _abi.MAT_J2_ISO
+STATUS_OK = _abi.STATUS_OK
+STATUS_INVALID = _abi.STATUS_INVALID
+STATUS_NOT_CONVERGED = _abi.STATUS_NOT_CONVERGED

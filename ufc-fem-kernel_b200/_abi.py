@@ -111,6 +111,23 @@ class NrArg(C.Structure):
                 ("lin_iters_total", _i32), ("residual_norm", _d), ("res_hist", _d * 32), ("status", _i32)]
 
 
+class StepArg(C.Structure):
+    _fields_ = [("u_prescribed_end", _p), ("f_ext_start", _p), ("f_ext_end", _p), ("mem", _i32),
+                ("time_period", _d), ("dt_initial", _d), ("dt_min", _d), ("dt_max", _d),
+                ("max_increments", _i32), ("max_cutbacks", _i32), ("auto_dt", _i32), ("target_iters", _i32),
+                ("growth_threshold", _d), ("growth_factor", _d), ("cutback_factor", _d),
+                ("max_iterations", _i32), ("tolerance_force", _d), ("lin", SolverAlgo),
+                ("hist_time", _p), ("hist_dt", _p), ("hist_iters", _p), ("hist_converged", _p),
+                ("hist_cap", _i32), ("attempts", _i32), ("increments", _i32), ("cutbacks", _i32),
+                ("nr_iterations", _i32), ("lin_iters_total", _i64), ("final_time", _d), ("completed", _i32),
+                ("status", _i32)]
+
+
+class FaceLoadArg(C.Structure):
+    _fields_ = [("n_faces", _i32), ("elem", _p), ("face", _p), ("traction", _p), ("pressure", _p),
+                ("index_base", _i32), ("mem", _i32), ("f", _p)]
+
+
 class TimingInfo(C.Structure):
     _fields_ = [("spmv_launches", _i32), ("spmv_ms", _d), ("spmv_bytes", _i64), ("precision", _i32),
                 ("kernel_launches", _i64)]
@@ -137,6 +154,10 @@ _SIGS = {
     "ufc_last_timing": [_p, C.POINTER(TimingInfo)],
     "ufc_last_residual_history": [_p, _p, _i32, C.POINTER(_i32)],
     "ufc_nr_increment": [_p, C.POINTER(NrArg)],
+    "ufc_nr_step": [_p, C.POINTER(StepArg)],
+    "ufc_load_faces": [_p, C.POINTER(FaceLoadArg)],
+    "ufc_stress_nodal": [_p, _p, _p, _p, _i32],
+    "ufc_reactions": [_p, _p, _p, _p, _i32],
     "ufc_state_commit": [_p],
     "ufc_state_rollback": [_p],
     "ufc_get_displacement": [_p, _p, _i32],

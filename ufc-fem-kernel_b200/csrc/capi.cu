@@ -192,6 +192,21 @@ __global__ void k_axpy(int64_t n, double a, const double* __restrict__ x, double
     y[i] += a * x[i];
 }
 
+// out = a + s (b - a), a or b NULL meaning zero.
+__global__ void k_lerp(int64_t n, const double* __restrict__ a, const double* __restrict__ b, double s,
+                       double* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double ai = a ? a[i] : 0.0, bi = b ? b[i] : 0.0;
+    out[i] = ai + s * (bi - ai);
+  }
+}
+
+__global__ void k_gather_dofs(int32_t nfix, const int32_t* __restrict__ dofs, const double* __restrict__ u,
+                              double* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nfix) out[i] = u[dofs[i]];
+}
+
 }  // namespace
 }  // namespace ufc
 
@@ -498,6 +513,64 @@ int ufc_stress_eval(ufc_ctx* c, const double* u, double* sig, double* vm, int32_
   return sync(c);
 }
 
+int ufc_load_faces(ufc_ctx* c, const ufc_face_load_arg* a) {
+  CTX_CHECK(c);
+  if (!a || !a->f || a->n_faces < 0 || (a->n_faces > 0 && (!a->elem || !a->face)))
+    return fail(c, UFC_STATUS_INVALID, "ufc_load_faces: NULL arrays");
+  if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_load_faces: pattern not built");
+  if (a->index_base != 0 && a->index_base != 1) return fail(c, UFC_STATUS_INVALID, "ufc_load_faces: index_base");
+  Scope sc(c);
+  const int32_t nf = a->n_faces;
+  std::vector<int32_t> he(nf), hf(nf);
+  if (nf > 0) {
+    const cudaMemcpyKind k = a->mem == UFC_MEM_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
+    UFC_CUDA(c, cudaMemcpyAsync(he.data(), a->elem, sizeof(int32_t) * nf, k, c->stream));
+    UFC_CUDA(c, cudaMemcpyAsync(hf.data(), a->face, sizeof(int32_t) * nf, k, c->stream));
+    UFC_TRY(sync(c));
+  }
+  for (int32_t i = 0; i < nf; ++i) {
+    he[i] -= a->index_base;
+    if (he[i] < 0 || he[i] >= c->E) return fail(c, UFC_STATUS_INVALID, "ufc_load_faces: element id out of range");
+    if (hf[i] < 1 || hf[i] > 6) return fail(c, UFC_STATUS_INVALID, "ufc_load_faces: face id must be 1..6");
+  }
+  Staged<double> st, sp, sf;
+  UFC_TRY(stage_in(c, st, a->traction, (int64_t)nf * 3, a->mem));
+  UFC_TRY(stage_in(c, sp, a->pressure, nf, a->mem));
+  UFC_TRY(stage_out(c, sf, a->f, c->n, a->mem));
+  UFC_TRY(face_loads(c, nf, he.data(), hf.data(), st.dev, sp.dev, sf.dev));
+  UFC_TRY(finish(c, sf));
+  return sync(c);
+}
+
+int ufc_stress_nodal(ufc_ctx* c, const double* u, double* sig, double* vm, int32_t mem) {
+  CTX_CHECK(c);
+  if (!c->has_material || !c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_stress_nodal: model not set up");
+  Scope sc(c);
+  Staged<double> su, ss, sv;
+  UFC_TRY(stage_in(c, su, u, c->n, mem));
+  UFC_TRY(stage_out(c, ss, sig, (int64_t)c->N * 6, mem));
+  UFC_TRY(stage_out(c, sv, vm, c->N, mem));
+  UFC_TRY(stress_nodal(c, su.dev ? su.dev : c->u, ss.dev, sv.dev));
+  UFC_TRY(finish(c, ss));
+  UFC_TRY(finish(c, sv));
+  return sync(c);
+}
+
+int ufc_reactions(ufc_ctx* c, const double* u, const double* f_ext, double* rf, int32_t mem) {
+  CTX_CHECK(c);
+  if (!rf) return fail(c, UFC_STATUS_INVALID, "ufc_reactions: NULL rf");
+  if (!c->has_material || !c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_reactions: model not set up");
+  Scope sc(c);
+  Staged<double> su, se, sr;
+  UFC_TRY(stage_in(c, su, u, c->n, mem));
+  UFC_TRY(stage_in(c, se, f_ext, c->n, mem));
+  UFC_TRY(stage_out(c, sr, rf, c->nfix, mem));
+  UFC_TRY(reactions(c, su.dev ? su.dev : c->u, se.dev, sr.dev));
+  UFC_TRY(finish(c, sr));
+  UFC_TRY(sync(c));
+  return check_dev_err(c, "ufc_reactions");
+}
+
 int ufc_spmv(ufc_ctx* c, int32_t precision, const void* x, void* y, int32_t mem) {
   CTX_CHECK(c);
   if (!x || !y) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: NULL vector");
@@ -629,7 +702,11 @@ int ufc_nr_increment(ufc_ctx* c, ufc_nr_arg* a) {
     const double ref = std::max({std::sqrt(c->h_scal->nr_ee), std::sqrt(c->h_scal->nr_ff), 1e-30});
     a->res_hist[it] = rn / ref;
     a->residual_norm = rn / ref;
-    if (!std::isfinite(rn)) return fail(c, UFC_STATUS_ERROR, "ufc_nr_increment: non-finite residual");
+    if (!std::isfinite(rn)) {  // a diverged iterate: a non-convergence the step driver cuts back on
+      a->iterations = it;
+      a->status = UFC_STATUS_NOT_CONVERGED;
+      return fail(c, UFC_STATUS_NOT_CONVERGED, "ufc_nr_increment: non-finite residual");
+    }
     if (!lift && rn <= a->tolerance_force * ref) {
       a->converged = 1;
       a->iterations = it;
@@ -660,6 +737,110 @@ int ufc_nr_increment(ufc_ctx* c, ufc_nr_arg* a) {
   a->status = a->converged ? UFC_STATUS_OK : UFC_STATUS_NOT_CONVERGED;
   if (!a->converged) fail(c, UFC_STATUS_NOT_CONVERGED, "ufc_nr_increment: Newton-Raphson did not converge");
   return a->status;
+}
+
+int ufc_nr_step(ufc_ctx* c, ufc_step_arg* a) {
+  CTX_CHECK(c);
+  if (!a) return fail(c, UFC_STATUS_INVALID, "ufc_nr_step: NULL arg");
+  if (!c->has_pattern || !c->has_material) return fail(c, UFC_STATUS_INVALID, "ufc_nr_step: model not set up");
+  if (!(a->time_period > 0.0) || !(a->dt_initial > 0.0) || !(a->dt_min > 0.0) || a->dt_max < a->dt_min ||
+      a->max_increments <= 0 || a->max_cutbacks < 0 || !(a->cutback_factor > 0.0 && a->cutback_factor < 1.0) ||
+      !(a->growth_factor >= 1.0) || a->max_iterations <= 0 || a->max_iterations > 32 || a->hist_cap < 0)
+    return fail(c, UFC_STATUS_INVALID, "ufc_nr_step: invalid increment controls");
+  Scope sc(c);
+  a->attempts = a->increments = a->cutbacks = a->nr_iterations = 0;
+  a->lin_iters_total = 0;
+  a->final_time = 0.0;
+  a->completed = 0;
+  Staged<double> ue, fs, fe;
+  UFC_TRY(stage_in(c, ue, a->u_prescribed_end, c->nfix, a->mem));
+  UFC_TRY(stage_in(c, fs, a->f_ext_start, c->n, a->mem));
+  UFC_TRY(stage_in(c, fe, a->f_ext_end, c->n, a->mem));
+  // prescribed values at the start of the step: those of the committed displacement
+  double *u0 = nullptr, *ut = nullptr, *ft = nullptr;
+  auto cleanup = [&]() {
+    if (u0) cudaFreeAsync(u0, c->stream);
+    if (ut) cudaFreeAsync(ut, c->stream);
+    if (ft) cudaFreeAsync(ft, c->stream);
+  };
+  const int64_t nf = std::max<int32_t>(c->nfix, 1);
+  if (cudaMallocAsync((void**)&u0, sizeof(double) * nf, c->stream) != cudaSuccess ||
+      cudaMallocAsync((void**)&ut, sizeof(double) * nf, c->stream) != cudaSuccess ||
+      cudaMallocAsync((void**)&ft, sizeof(double) * c->n, c->stream) != cudaSuccess) {
+    cleanup();
+    return fail(c, UFC_STATUS_MEM_ERROR, "ufc_nr_step: cudaMallocAsync failed");
+  }
+  if (c->nfix > 0)
+    k_gather_dofs<<<grid_for(c->nfix, 256), 256, 0, c->stream>>>(c->nfix, c->fix_dofs, c->u_n, u0);
+  const double T = a->time_period;
+  const double* uend = ue.dev ? ue.dev : u0;
+  const int vg = std::min(grid_for(c->n, 256), 148 * 8);
+  double t = 0.0, dt = std::min(a->dt_initial, a->dt_max);
+  int cut_run = 0, status = UFC_STATUS_OK;
+  while (t < T * (1.0 - 1e-12) && a->attempts < a->max_increments) {
+    dt = std::min(dt, T - t);
+    const double t1 = t + dt;
+    const double sfrac = t1 >= T ? 1.0 : t1 / T;
+    if (c->nfix > 0) k_lerp<<<grid_for(c->nfix, 256), 256, 0, c->stream>>>(c->nfix, u0, uend, sfrac, ut);
+    k_lerp<<<vg, 256, 0, c->stream>>>(c->n, fs.dev, fe.dev, sfrac, ft);
+    if (cudaGetLastError() != cudaSuccess) {
+      status = fail(c, UFC_STATUS_ERROR, "ufc_nr_step: launch failed");
+      break;
+    }
+    ufc_nr_arg na{};
+    na.u_prescribed = c->nfix > 0 ? ut : nullptr;
+    na.f_ext = ft;
+    na.mem = UFC_MEM_DEVICE;
+    na.max_iterations = a->max_iterations;
+    na.tolerance_force = a->tolerance_force;
+    na.lin = a->lin;
+    const int s = ufc_nr_increment(c, &na);
+    const int k = a->attempts++;
+    a->lin_iters_total += na.lin_iters_total;
+    const bool ok = s == UFC_STATUS_OK && na.converged;
+    if (k < a->hist_cap) {
+      if (a->hist_time) a->hist_time[k] = t1;
+      if (a->hist_dt) a->hist_dt[k] = dt;
+      if (a->hist_iters) a->hist_iters[k] = na.iterations;
+      if (a->hist_converged) a->hist_converged[k] = ok ? 1 : 0;
+    }
+    if (ok) {
+      status = ufc_state_commit(c);
+      if (status != UFC_STATUS_OK) break;
+      t = t1 >= T ? T : t1;
+      a->increments += 1;
+      a->nr_iterations += na.iterations;
+      cut_run = 0;
+      if (a->auto_dt && na.iterations <= (int)(a->target_iters * a->growth_threshold))
+        dt = std::min(dt * a->growth_factor, a->dt_max);
+      continue;
+    }
+    if (s != UFC_STATUS_NOT_CONVERGED) {  // not a convergence failure: report it as is
+      ufc_state_rollback(c);
+      status = s;
+      break;
+    }
+    status = ufc_state_rollback(c);
+    if (status != UFC_STATUS_OK) break;
+    a->cutbacks += 1;
+    if (++cut_run > a->max_cutbacks) {
+      status = fail(c, UFC_STATUS_NOT_CONVERGED, "ufc_nr_step: max cutbacks exceeded");
+      break;
+    }
+    dt *= a->cutback_factor;
+    if (dt < a->dt_min) {
+      status = fail(c, UFC_STATUS_NOT_CONVERGED, "ufc_nr_step: increment below dt_min");
+      break;
+    }
+  }
+  cleanup();
+  a->final_time = t;
+  a->completed = t >= T * (1.0 - 1e-12) ? 1 : 0;
+  if (status == UFC_STATUS_OK && !a->completed)
+    status = fail(c, UFC_STATUS_NOT_CONVERGED, "ufc_nr_step: max_increments reached before the end of the step");
+  a->status = status;
+  UFC_TRY(sync(c));
+  return status;
 }
 
 int ufc_state_commit(ufc_ctx* c) {

@@ -352,6 +352,7 @@ int build_pattern(Ctx* c) {
   // 1. colouring (host) and colour-grouped element lists
   std::vector<int32_t> color;
   UFC_TRY(color_elements(c, color));
+  c->h_color = color;
   c->col_off.assign(c->ncol + 1, 0);
   for (int32_t e = 0; e < E; ++e) c->col_off[color[e] + 1]++;
   for (int k = 0; k < c->ncol; ++k) c->col_off[k + 1] += c->col_off[k];

@@ -75,6 +75,7 @@ struct Ctx {
   int32_t ncol = 0;
   std::vector<int32_t> col_off;      // ncol+1
   int32_t* col_elems = nullptr;      // [E] elements grouped by colour, ascending inside a colour
+  std::vector<int32_t> h_color;      // [E] colour of each element (host)
 
   // pattern: canonical block CSR + SELL-32 storage
   bool has_pattern = false;
@@ -168,6 +169,12 @@ int mat_update_batch(Ctx* c, const ufc_mat_update_arg* a, const double* props, c
                      int32_t* yielded);
 int stress_eval(Ctx* c, const double* u, double* sig, double* vm);
 int adjoint_sens(Ctx* c, int nrhs, const double* U, const double* L, double* g);
+
+// output.cu
+int face_loads(Ctx* c, int32_t n_faces, const int32_t* h_elem, const int32_t* h_face, const double* traction,
+               const double* pressure, double* f);  // h_elem 0-based, h_face 1..6 (host); others device
+int stress_nodal(Ctx* c, const double* u, double* sig_node, double* vm_node);
+int reactions(Ctx* c, const double* u, const double* f_ext, double* rf);
 int build_dinv(Ctx* c, int precision);
 
 // spmv.cu

@@ -127,6 +127,21 @@ class SolverState:
 
 
 @dataclass
+class StepResult:
+    """Outcome of FemModel.nr_step; history rows are (step time, dt, Newton
+    iterations, converged) per attempted increment."""
+    completed: bool
+    final_time: float
+    increments: int
+    cutbacks: int
+    attempts: int
+    nr_iterations: int
+    lin_iters_total: int
+    history: list = field(default_factory=list)
+    status: int = 0
+
+
+@dataclass
 class NrResult:
     iterations: int
     converged: bool
@@ -362,6 +377,75 @@ class FemModel:
                        list(a.res_hist[: max(a.iterations + 1, 1)]))
         self._check(st, "ufc_nr_increment")
         return res
+
+    def nr_step(self, u_prescribed_end=None, f_ext_end=None, f_ext_start=None, time_period=1.0, dt_initial=1.0,
+                dt_min=1e-5, dt_max=1.0, max_increments=100, max_cutbacks=5, auto_dt=True, target_iters=6,
+                growth_threshold=0.8, growth_factor=1.25, cutback_factor=0.5, max_iterations=25,
+                tolerance_force=1e-8, lin: SolverAlgo | None = None, raise_on_failure=False):
+        """One step with automatic increments and cutbacks (ufc_nr_step); the
+        defaults are the reference's RT_Step_Stp_Ctl_Algo values."""
+        lin = lin or SolverAlgo()
+        ub = _Buf(u_prescribed_end, np.float64, self.fixed.size if u_prescribed_end is not None else None)
+        fsb = _Buf(f_ext_start, np.float64, self.n_dof if f_ext_start is not None else None)
+        feb = _Buf(f_ext_end, np.float64, self.n_dof if f_ext_end is not None else None)
+        cap = int(max_increments)
+        ht, hd = np.zeros(cap), np.zeros(cap)
+        hi, hc = np.zeros(cap, dtype=np.int32), np.zeros(cap, dtype=np.int32)
+        a = A.StepArg()
+        a.u_prescribed_end, a.f_ext_start, a.f_ext_end = ub.ptr, fsb.ptr, feb.ptr
+        a.mem = _same_mem(ub, fsb, feb)
+        a.time_period, a.dt_initial, a.dt_min, a.dt_max = time_period, dt_initial, dt_min, dt_max
+        a.max_increments, a.max_cutbacks, a.auto_dt, a.target_iters = cap, max_cutbacks, int(auto_dt), target_iters
+        a.growth_threshold, a.growth_factor, a.cutback_factor = growth_threshold, growth_factor, cutback_factor
+        a.max_iterations, a.tolerance_force, a.lin = max_iterations, tolerance_force, lin.to_c()
+        a.hist_time, a.hist_dt = ht.ctypes.data, hd.ctypes.data
+        a.hist_iters, a.hist_converged = hi.ctypes.data, hc.ctypes.data
+        a.hist_cap = cap
+        st = self.lib.ufc_nr_step(self.h, C.byref(a))
+        k = min(a.attempts, cap)
+        res = StepResult(bool(a.completed), a.final_time, a.increments, a.cutbacks, a.attempts, a.nr_iterations,
+                         a.lin_iters_total, [(float(ht[i]), float(hd[i]), int(hi[i]), bool(hc[i])) for i in range(k)],
+                         st)
+        if st != A.STATUS_NOT_CONVERGED or raise_on_failure:
+            self._check(st, "ufc_nr_step")
+        return res
+
+    def load_faces(self, elem, face, traction=None, pressure=None, index_base=0, out=None):
+        """Equivalent nodal forces of face tractions ([n_faces, 3]) and/or
+        pressures ([n_faces]) on the faces `face` (1..6) of elements `elem`."""
+        like = traction if traction is not None else (pressure if pressure is not None else elem)
+        n_faces = len(elem)
+        f = out if out is not None else self._empty(self.n_dof, np.float64, like if _is_torch(like) else np.zeros(1))
+        eb, fb = _Buf(elem, np.int32, n_faces), _Buf(face, np.int32, n_faces)
+        tb = _Buf(traction, np.float64, 3 * n_faces if traction is not None else None)
+        pb = _Buf(pressure, np.float64, n_faces if pressure is not None else None)
+        ob = _Buf(f, np.float64, self.n_dof, writable=True)
+        a = A.FaceLoadArg(n_faces, eb.ptr, fb.ptr, tb.ptr, pb.ptr, int(index_base), _same_mem(eb, fb, tb, pb, ob),
+                          ob.ptr)
+        self._check(self.lib.ufc_load_faces(self.h, C.byref(a)), "ufc_load_faces")
+        return f
+
+    def stress_nodal(self, u=None, want_sigma=True):
+        """Nodal stress [n_nodes, 6] (extrapolated from the Gauss points and
+        averaged over elements) and its von Mises value [n_nodes]."""
+        like = u if u is not None else np.zeros(1)
+        sig = self._empty(self.n_nodes * 6, np.float64, like) if want_sigma else None
+        vm = self._empty(self.n_nodes, np.float64, like)
+        ub = _Buf(u, np.float64, self.n_dof if u is not None else None)
+        sb, vb = _Buf(sig, np.float64, writable=True), _Buf(vm, np.float64, writable=True)
+        self._check(self.lib.ufc_stress_nodal(self.h, ub.ptr, sb.ptr, vb.ptr, _same_mem(ub, sb, vb)),
+                    "ufc_stress_nodal")
+        return (sig.reshape(self.n_nodes, 6) if sig is not None else None), vm
+
+    def reactions(self, u=None, f_ext=None):
+        """RF = F_int(u) - F_ext at the prescribed DOFs, in the order of set_bc."""
+        like = u if u is not None else (f_ext if f_ext is not None else np.zeros(1))
+        rf = self._empty(max(self.fixed.size, 1), np.float64, like)
+        ub = _Buf(u, np.float64, self.n_dof if u is not None else None)
+        fb = _Buf(f_ext, np.float64, self.n_dof if f_ext is not None else None)
+        rb = _Buf(rf, np.float64, writable=True)
+        self._check(self.lib.ufc_reactions(self.h, ub.ptr, fb.ptr, rb.ptr, _same_mem(ub, fb, rb)), "ufc_reactions")
+        return rf[: self.fixed.size]
 
     def commit(self):
         self._check(self.lib.ufc_state_commit(self.h), "ufc_state_commit")
