@@ -91,10 +91,34 @@ MODULE ufc_gpu_brg
     INTEGER(C_INT32_T)    :: status
   END TYPE
 
+  TYPE, BIND(C), PUBLIC :: ufc_step_arg             ! RT_StepDriver_Execute, one step with cutbacks
+    TYPE(C_PTR)           :: u_prescribed_end, f_ext_start, f_ext_end
+    INTEGER(C_INT32_T)    :: mem
+    REAL(C_DOUBLE)        :: time_period = 1.0D0, dt_initial = 1.0D0, dt_min = 1.0D-5, dt_max = 1.0D0
+    INTEGER(C_INT32_T)    :: max_increments = 100, max_cutbacks = 5, auto_dt = 1, target_iters = 6
+    REAL(C_DOUBLE)        :: growth_threshold = 0.8D0, growth_factor = 1.25D0, cutback_factor = 0.5D0
+    INTEGER(C_INT32_T)    :: max_iterations = 25
+    REAL(C_DOUBLE)        :: tolerance_force = 1.0D-8
+    TYPE(ufc_solver_algo) :: lin
+    TYPE(C_PTR)           :: hist_time, hist_dt, hist_iters, hist_converged
+    INTEGER(C_INT32_T)    :: hist_cap = 0, attempts, increments, cutbacks, nr_iterations
+    INTEGER(C_INT64_T)    :: lin_iters_total
+    REAL(C_DOUBLE)        :: final_time
+    INTEGER(C_INT32_T)    :: completed, status
+  END TYPE
+
+  TYPE, BIND(C), PUBLIC :: ufc_face_load_arg        ! PH_Elem_C3D8_FormFacePressure over a face set
+    INTEGER(C_INT32_T)    :: n_faces
+    TYPE(C_PTR)           :: elem, face, traction, pressure
+    INTEGER(C_INT32_T)    :: index_base, mem
+    TYPE(C_PTR)           :: f
+  END TYPE
+
   PUBLIC :: ufc_ctx_create, ufc_ctx_destroy, ufc_last_error, ufc_mesh_set, ufc_material_set, ufc_bc_set
   PUBLIC :: ufc_pattern_build, ufc_csr_export, ufc_elem_compute_ke, ufc_elem_compute_fint
   PUBLIC :: ufc_mat_update_batch, ufc_pcg_solve, ufc_pcg_solve_block, ufc_nr_increment
   PUBLIC :: ufc_state_commit, ufc_state_rollback, ufc_get_displacement, ufc_adjoint_sensitivity
+  PUBLIC :: ufc_nr_step, ufc_load_faces, ufc_stress_nodal, ufc_reactions
 
   INTERFACE
     INTEGER(C_INT) FUNCTION ufc_ctx_create(device, ctx) BIND(C, NAME='ufc_ctx_create')
@@ -176,6 +200,26 @@ MODULE ufc_gpu_brg
       IMPORT :: C_INT, C_PTR, ufc_nr_arg
       TYPE(C_PTR), VALUE               :: ctx
       TYPE(ufc_nr_arg), INTENT(INOUT)  :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_nr_step(ctx, arg) BIND(C, NAME='ufc_nr_step')
+      IMPORT :: C_INT, C_PTR, ufc_step_arg
+      TYPE(C_PTR), VALUE                 :: ctx
+      TYPE(ufc_step_arg), INTENT(INOUT)  :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_load_faces(ctx, arg) BIND(C, NAME='ufc_load_faces')
+      IMPORT :: C_INT, C_PTR, ufc_face_load_arg
+      TYPE(C_PTR), VALUE                  :: ctx
+      TYPE(ufc_face_load_arg), INTENT(IN) :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_stress_nodal(ctx, u, stress_node, vm_node, mem) BIND(C, NAME='ufc_stress_nodal')
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx, u, stress_node, vm_node   ! C_NULL_PTR where not wanted
+      INTEGER(C_INT32_T), VALUE     :: mem
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_reactions(ctx, u, f_ext, rf, mem) BIND(C, NAME='ufc_reactions')
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx, u, f_ext, rf              ! u, f_ext may be C_NULL_PTR
+      INTEGER(C_INT32_T), VALUE     :: mem
     END FUNCTION
     INTEGER(C_INT) FUNCTION ufc_state_commit(ctx) BIND(C, NAME='ufc_state_commit')
       IMPORT :: C_INT, C_PTR

@@ -4,12 +4,14 @@
 //
 // Vectors are interleaved, entry (dof i, rhs k) at i*nr + k with nr the number
 // of right-hand sides rounded up to a power of two (<= 32; padded columns are
-// zero and inactive).  A thread owns G = min(nr, 8) consecutive right-hand
-// sides of one block row: it loads each stored 3x3 block once (the threads of
-// a warp cover 32/tpr consecutive rows of a SELL slice, tpr = nr/G threads per
-// row, so every value load is one coalesced line) and the G entries of each x
-// component with 16-byte loads, keeping 3*G row sums in registers.  The vector
-// kernels give every thread the same G right-hand sides of successive dofs.
+// zero and inactive).  A thread owns G = min(nr, 2) consecutive right-hand
+// sides of one block row, so the tpr = nr/G threads of a row read the nr
+// entries of one x component (nr*8 contiguous bytes, a full 128-byte line for
+// 16 right-hand sides) with one 16-byte load each: every x load of a warp
+// touches 32/tpr lines, each in full, which keeps the L1 wavefronts per byte
+// low; the 9 values of a stored block are loaded once per thread (the lanes of
+// a row share them) and the row sums stay in registers.  The vector kernels
+// give every thread the same G right-hand sides of successive dofs.
 // Each right-hand side has its own alpha, beta and stop test; a converged
 // right-hand side is frozen (alpha = beta = 0) while the others continue.
 // Reductions are per right-hand side and deterministic: lanes that hold the
@@ -146,7 +148,7 @@ __device__ bool rhs_grid_sum(double (&v)[NV][G], int tpr, int nr, double* __rest
 // y = K x for nr interleaved vectors (FP64 SELL values); MODE 1 also forms
 // p.q per rhs and alpha.  One warp task = 32/tpr rows of a slice.
 template <int G, int MODE>
-__global__ void __launch_bounds__(kBlk, 2)
+__global__ void __launch_bounds__(kBlk, 4)
     k_bspmv(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
             const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y, int nr, int tpr,
             BScalars* __restrict__ s, double* __restrict__ partials) {
@@ -173,6 +175,7 @@ __global__ void __launch_bounds__(kBlk, 2)
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int i = 0; i < G; ++i) acc[r][i] = 0.0;
+#pragma unroll 2
     for (int j = 0; j < len; ++j) {
       const int64_t cj = __ldcs(cp + 32 * j);
       const double* v = vp + 288 * (int64_t)j;
@@ -522,7 +525,7 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* Bm, double* X, const ufc_sol
     return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: method must be CG and max_iter > 0");
   int nr = 1;
   while (nr < nrhs) nr <<= 1;
-  const int G = std::min(nr, 8);
+  const int G = std::min(nr, 2);
   BlockRun B{};
   B.c = c;
   B.nr = nr;
@@ -579,12 +582,10 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* Bm, double* X, const ufc_sol
 
   std::vector<double> tol(nr, 0.0), bnorm(nr, 1.0);
   std::vector<int> n_refine(nr, 0);
-  switch (G) {
-    case 1: status = pcg_block_run<1>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st); break;
-    case 2: status = pcg_block_run<2>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st); break;
-    case 4: status = pcg_block_run<4>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st); break;
-    default: status = pcg_block_run<8>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st); break;
-  }
+  if (G == 1)
+    status = pcg_block_run<1>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st);
+  else
+    status = pcg_block_run<2>(B, nrhs, algo, hs, restart_dev, bnorm, tol, n_refine, st);
   if (status != UFC_STATUS_OK) {
     cleanup();
     return status;

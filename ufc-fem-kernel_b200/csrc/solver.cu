@@ -46,18 +46,76 @@ int vec_grid(int64_t n) {
 
 enum SpmvMode { kPlain = 0, kCg = 1 };
 
-// y = K x over SELL-32 slices: one thread per block row, SPLIT warps per slice.
-// With SPLIT > 1 the warps of a slice take the stored blocks j = part,
-// part + SPLIT, ... of their 32 rows (every load stays a coalesced 32-row
-// line) and their partial row sums are added in shared memory in warp order,
-// so the result depends only on SPLIT, which the launcher derives from the
-// problem size (more warps in flight for meshes with few slices per SM).
+// y = K x, one thread per block row of a SELL-32 slice (a warp = a slice).
 // TV: stored value type, TX: vector type, TA: accumulator type of the row sums.
 // DIFF: values in difference form (diagonal slot = block row sum S_i), so the
 // row is evaluated as sum_{j != i} K_ij (x_j - x_i) + S_i x_i.
+template <typename TV, typename TX, typename TA, int MODE, bool DIFF>
+__global__ void __launch_bounds__(kSpmvBlock)
+    k_spmv(int32_t N, int64_t nrows_pad, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
+           const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y, CgScalars* __restrict__ scal,
+           double* __restrict__ partials) {
+  if (MODE == kCg && scal->stop) return;
+  const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
+  double dot[1] = {0.0};
+  if (row < nrows_pad) {
+    const int64_t s = row >> 5;
+    const int t = (int)(row & 31);
+    const int64_t base = sptr[s];
+    const int len = (int)((sptr[s + 1] - base) >> 5);
+    const int32_t* cp = col + base + t;
+    const TV* vp = val + 9 * base + t;
+    TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
+    TA xi0 = TA(0), xi1 = TA(0), xi2 = TA(0);
+    if (DIFF && row < N) {
+      xi0 = (TA)x[3 * row];
+      xi1 = (TA)x[3 * row + 1];
+      xi2 = (TA)x[3 * row + 2];
+    }
+#pragma unroll 2
+    for (int j = 0; j < len; ++j) {
+      const int64_t cj = __ldcs(cp + 32 * j);
+      TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
+      if (DIFF && cj != row) {
+        x0 -= xi0;
+        x1 -= xi1;
+        x2 -= xi2;
+      }
+      const TV* v = vp + 288 * (int64_t)j;
+      a0 += (TA)__ldcs(v) * x0 + (TA)__ldcs(v + 32) * x1 + (TA)__ldcs(v + 64) * x2;
+      a1 += (TA)__ldcs(v + 96) * x0 + (TA)__ldcs(v + 128) * x1 + (TA)__ldcs(v + 160) * x2;
+      a2 += (TA)__ldcs(v + 192) * x0 + (TA)__ldcs(v + 224) * x1 + (TA)__ldcs(v + 256) * x2;
+    }
+    if (row < N) {
+      y[3 * row] = (TX)a0;
+      y[3 * row + 1] = (TX)a1;
+      y[3 * row + 2] = (TX)a2;
+      if (MODE == kCg)
+        dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
+    }
+  }
+  if (MODE == kCg) {
+    double tot[1];
+    if (grid_sum<1>(dot, partials, &scal->ticket[0], tot)) {
+      scal->pq = tot[0];
+      if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
+        scal->stop = 3;
+      } else {
+        scal->alpha = scal->rz / tot[0];
+      }
+    }
+  }
+}
+
+// The same product with SPLIT (2, 4 or 8) warps per slice, for meshes with few
+// slices per SM: the warps of a slice take the stored blocks j = part,
+// part + SPLIT, ... of their 32 rows (every load stays a coalesced 32-row
+// line) and their partial row sums are added in shared memory in warp order,
+// so the result depends only on SPLIT, which the launcher derives from the
+// problem size.
 template <typename TV, typename TX, typename TA, int MODE, bool DIFF, int SPLIT>
 __global__ void __launch_bounds__(kSpmvBlock)
-    k_spmv(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
+    k_spmv_split(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
            const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y, CgScalars* __restrict__ scal,
            double* __restrict__ partials) {
   if (MODE == kCg && scal->stop) return;
@@ -78,8 +136,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
       xi1 = (TA)x[3 * row + 1];
       xi2 = (TA)x[3 * row + 2];
     }
-#pragma unroll 2
-    for (int j = part; j < len; j += SPLIT) {
+    auto block = [&](int j) {
       const int64_t cj = __ldcs(cp + 32 * j);
       TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
       if (DIFF && cj != row) {
@@ -91,9 +148,11 @@ __global__ void __launch_bounds__(kSpmvBlock)
       a0 += (TA)__ldcs(v) * x0 + (TA)__ldcs(v + 32) * x1 + (TA)__ldcs(v + 64) * x2;
       a1 += (TA)__ldcs(v + 96) * x0 + (TA)__ldcs(v + 128) * x1 + (TA)__ldcs(v + 160) * x2;
       a2 += (TA)__ldcs(v + 192) * x0 + (TA)__ldcs(v + 224) * x1 + (TA)__ldcs(v + 256) * x2;
-    }
+    };
+#pragma unroll 2
+    for (int j = part; j < len; j += SPLIT) block(j);
   }
-  if constexpr (SPLIT > 1) {
+  {
     __shared__ TA sh[kWarps][3][32];
     sh[warp][0][lane] = a0;
     sh[warp][1][lane] = a1;
@@ -144,10 +203,16 @@ int spmv_split(const Ctx* c) {
 
 template <typename TV, typename TX, typename TA, int MODE, bool DIFF, int SPLIT>
 void launch_spmv_split(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
-  constexpr int per_block = kSpmvBlock / 32 / SPLIT;
-  const int grid = (int)((c->nslices + per_block - 1) / per_block);
-  k_spmv<TV, TX, TA, MODE, DIFF, SPLIT><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices, c->slice_ptr, c->sell_col,
-                                                                      val, x, y, c->scal, c->partials);
+  if constexpr (SPLIT == 1) {
+    const int grid = (int)((c->nslices * kSlice + kSpmvBlock - 1) / kSpmvBlock);
+    k_spmv<TV, TX, TA, MODE, DIFF><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->slice_ptr,
+                                                                c->sell_col, val, x, y, c->scal, c->partials);
+  } else {
+    constexpr int per_block = kSpmvBlock / 32 / SPLIT;
+    const int grid = (int)((c->nslices + per_block - 1) / per_block);
+    k_spmv_split<TV, TX, TA, MODE, DIFF, SPLIT><<<grid, kSpmvBlock, 0, st>>>(
+        c->N, c->nslices, c->slice_ptr, c->sell_col, val, x, y, c->scal, c->partials);
+  }
 }
 
 template <typename TV, typename TX, typename TA, int MODE, bool DIFF>

@@ -233,9 +233,9 @@ class FemModel:
                 "n_colors": info.n_colors, "max_row_blocks": info.max_row_blocks}
 
     @classmethod
-    def from_problem(cls, p, device=0, build_pattern=True):
+    def from_problem(cls, p, device=0, build_pattern=True, lib=None):
         """Model of a `mesh.Problem` (mesh, material, Dirichlet set)."""
-        m = cls(device)
+        m = cls(device, lib=lib)
         m.set_mesh(p.coords, p.conn)
         m.set_material(p.mat_model_id, p.props)
         m.set_bc(p.fixed, p.fixed_values)
