@@ -4,7 +4,9 @@ One step = one linear static solve K u = f on one GPU, from x0 = 0 to
 ||f - K u||_2 <= 1e-10 ||f||_2 in FP64, with the stiffness already assembled in
 HBM (pattern and assembly are timed separately and reported in `assembly`).
 The headline (`value`) is the FP32 matrix / FP64-refined PCG; the plain FP64
-PCG on the same mesh is timed in the same run (`fp64_path`).
+PCG on the same mesh is timed in the same run (`fp64_path`).  Both use the
+symmetric half storage of the block matrix by default (`--storage full` for
+the full SELL-32 storage, which is also timed once as `other_storage`).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU (torchrun, one rank per GPU): every rank solves its own copy of the
@@ -54,6 +56,8 @@ def parse(argv=None):
                     help="skip the J2 bar and adjoint block workloads reported under `other_configs`")
     ap.add_argument("--cpu-iters", type=int, default=12, help="CG iterations per CPU sample")
     ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--storage", choices=["symmetric", "full"], default="symmetric",
+                    help="block storage of both paths: symmetric half (default) or full SELL-32")
     return ap.parse_args(argv)
 
 
@@ -320,9 +324,12 @@ def run_ours(args):
     ev[1].record(stream)
     torch.cuda.synchronize(dev)
     pattern_ms = ev[0].elapsed_time(ev[1])
+    sym = args.storage == "symmetric"
+    build = ufc.BUILD_FP64 | ufc.BUILD_FP32_ROUNDED | (ufc.BUILD_SYMMETRIC if sym else 0)
     asm_ms = m.assemble(ufc.BUILD_FP64 | ufc.BUILD_FP32_ROUNDED)
     asm32_ms = m.assemble(ufc.BUILD_FP32)  # FP32 element kernel, timed for the elements/s figure
     asm_ms = m.assemble(ufc.BUILD_FP64 | ufc.BUILD_FP32_ROUNDED)
+    build_ms = m.assemble(build)
 
     b_host = ufc.lifted_rhs(m, p.f)
     b = torch.from_numpy(b_host).to(dev)
@@ -359,7 +366,8 @@ def run_ours(args):
     spmv_avg_s = tm["spmv_ms"] / tm["spmv_launches"] / 1e3
     peak, peak_kind = load_peaks()
     achieved = tm["spmv_bytes"] / spmv_avg_s / 1e9
-    traffic = profile_traffic("spmv_sell_fp32_192x96x96.txt")
+    traffic = profile_traffic("spmv_sym_fp32_192x96x96.txt" if sym else "spmv_sell_fp32_192x96x96.txt")
+    full_bytes32 = 40 * info["nnzb"] + 4 * (p.n_nodes + 1) + 8 * info["n_dof"]  # full block-CSR product, FP32
 
     # ---- plain FP64 PCG on the same mesh
     m.solve(b, fp64, x=x)
@@ -397,6 +405,31 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     t_e2e = max_over_ranks(e_ev[0].elapsed_time(e_ev[1]) / e_steps / 1e3, dev)
 
+    # ---- the other storage on the same mesh, one solve of each path
+    other = None
+    if sym:
+        m.assemble(ufc.BUILD_FP64 | ufc.BUILD_FP32_ROUNDED)
+        o = {}
+        for key, algo in (("mixed", mixed), ("fp64", fp64)):
+            m.solve(b, algo, x=x)
+            o_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            o_ev[0].record(stream)
+            _, ost = m.solve(b, algo, x=x)
+            o_ev[1].record(stream)
+            torch.cuda.synchronize(dev)
+            o[key] = max_over_ranks(o_ev[0].elapsed_time(o_ev[1]) / 1e3, dev)
+            o[key + "_iters"] = ost.niter
+        m.set_instrument(True)
+        m.solve(b, mixed, x=x)
+        tmf = m.last_timing()
+        m.set_instrument(False)
+        f_us = tmf["spmv_ms"] / tmf["spmv_launches"] * 1e3
+        other = {"storage": "full SELL-32 block CSR", "value": o["mixed"], "iters": o["mixed_iters"],
+                 "fp64_value": o["fp64"], "fp64_iters": o["fp64_iters"], "unit": UNIT,
+                 "spmv_us": f_us, "spmv_achieved_gbs": tmf["spmv_bytes"] / f_us / 1e3,
+                 "spmv_frac": tmf["spmv_bytes"] / f_us / 1e3 / peak,
+                 "traffic": profile_traffic("spmv_sell_fp32_192x96x96.txt")}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         setup, per, threads = cpu_sample(p, args.cpu_iters)
@@ -415,9 +448,12 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "mesh": args.mesh, "n_dof": info["n_dof"], "nnz": info["nnz"],
                    "nnzb": info["nnzb"], "sell_blocks": info["sell_blocks"],
                    "parallelism": "replicas" if world > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (FP32 matrix 1.93 GB per SpMV)",
-                   "solver": "Jacobi-PCG, FP32 SELL-BSR3 matrix rounded from FP64 assembly, FP32 vectors and "
-                             "row sums, FP64 x, FP64 matrix-free residual replacement (delta 0.1)"},
+                   "l2": "inputs larger than L2 (FP32 matrix 1.23 GB symmetric / 1.93 GB full per SpMV)",
+                   "storage": args.storage,
+                   "solver": "Jacobi-PCG, FP32 SELL-BSR3 matrix rounded from FP64 assembly"
+                             + (", symmetric half storage" if sym else "")
+                             + ", FP32 vectors and row sums, FP64 x, FP64 matrix-free residual replacement "
+                               "(delta 0.1); the FP64 path uses the same storage"},
         "iters": mean([s.niter for s in states]), "refinements": mean([s.n_refine for s in states]),
         "rnorm": max(s.rnorm for s in states),
         "dof_iterations_per_s": world * info["n_dof"] * mean([s.niter for s in states]) / t_mixed,
@@ -427,17 +463,24 @@ def run_ours(args):
         "speedup_vs_fp64": t_fp64 / t_mixed,
         "accuracy_vs_fp64_gpu": {"u_rel_l2": du, "von_mises_rel_max": dvm},
         "assembly": {"pattern_ms": pattern_ms, "fp64_plus_rounded_fp32_ms": asm_ms, "fp32_element_ms": asm32_ms,
+                     "with_storage_ms": build_ms,
                      "elements_per_s_fp32": p.n_elems / (asm32_ms / 1e3), "host_setup_s": setup_s},
-        "roofline": {"bound": "hbm", "kernel": "k_spmv<float,float,float,kCg> (SELL-32 BSR3 SpMV + p.Ap)",
+        "roofline": {"bound": "hbm",
+                     "kernel": ("k_spmv_sym<float,float,float,kCg> (symmetric SELL-32 BSR3 SpMV + p.Ap)" if sym else
+                                "k_spmv<float,float,float,kCg> (SELL-32 BSR3 SpMV + p.Ap)"),
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": tm["spmv_bytes"], "avg_launch_us": spmv_avg_s * 1e6,
-                     "launches_timed": tm["spmv_launches"]},
+                     "launches_timed": tm["spmv_launches"],
+                     "full_storage_bytes_per_launch": full_bytes32,
+                     "full_storage_equivalent_gbs": full_bytes32 / spmv_avg_s / 1e9},
         "e2e": {"value": t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * p.n_dof, "d2h_bytes_per_step": 8 * p.n_dof,
                 "api": "ufc_pcg_solve(mem=UFC_MEM_HOST) via FemModel.solve on pinned host buffers"},
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if other:
+        line["other_storage"] = other
     if cpu:
         line["cpu_baseline"] = cpu
     if not args.no_extras and world == 1:

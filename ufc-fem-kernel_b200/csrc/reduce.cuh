@@ -37,7 +37,14 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* sh) {
 // Grid-wide sum: every block calls it once with its per-thread values.  Returns
 // true in thread 0 of the last block to finish, whose `out` then holds the
 // total; the ticket is reset for the next launch.
-template <int NV>
+//
+// WIDE: the last block, which runs alone, keeps eight independent loads of
+// partials in flight per thread instead of one (summed in a fixed order).  It
+// shortens the tail of launches with thousands of blocks, but the extra code
+// also changes how the compiler schedules the caller's main loop: the fused
+// SpMV of the CG is faster with it for FP32 symmetric storage and slower for
+// the FP64 and full-storage kernels, as measured on B200, so the caller picks.
+template <int NV, bool WIDE = false>
 __device__ __forceinline__ bool grid_sum(double (&v)[NV], double* __restrict__ partials, uint32_t* ticket,
                                          double (&out)[NV]) {
   __shared__ double sh[32 * NV];
@@ -54,11 +61,36 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NV], double* __restrict__ p
   if (!last) return false;
   __threadfence();
   double acc[NV];
+  if constexpr (WIDE) {
+    constexpr int kU = 8;
+    double part[kU][NV];
 #pragma unroll
-  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-  for (int64_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    for (int u = 0; u < kU; ++u)
 #pragma unroll
-    for (int k = 0; k < NV; ++k) acc[k] += __ldcg(partials + b * NV + k);
+      for (int k = 0; k < NV; ++k) part[u][k] = 0.0;
+    const int64_t nb = gridDim.x, step = blockDim.x;
+    int64_t b = threadIdx.x;
+    for (; b + (kU - 1) * step < nb; b += kU * step)
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) part[u][k] += __ldcg(partials + (b + u * step) * NV + k);
+    for (; b < nb; b += step)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) part[0][k] += __ldcg(partials + b * NV + k);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      acc[k] = part[0][k];
+#pragma unroll
+      for (int u = 1; u < kU; ++u) acc[k] += part[u][k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int64_t b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) acc[k] += __ldcg(partials + b * NV + k);
+  }
   block_sum<NV>(acc, sh);
   if (threadIdx.x == 0) {
 #pragma unroll

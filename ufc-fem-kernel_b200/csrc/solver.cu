@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
   }
   if (MODE == kCg) {
     double tot[1];
-    if (grid_sum<1>(dot, partials, &scal->ticket[0], tot)) {
+    if (grid_sum<1, sizeof(TV) == 4>(dot, partials, &scal->ticket[0], tot)) {
       scal->pq = tot[0];
       if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
         scal->stop = 3;
