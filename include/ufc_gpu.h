@@ -61,6 +61,8 @@ extern "C" {
 #define UFC_SOLV_METHOD_CG 3
 #define UFC_SOLV_PREC_NONE 0
 #define UFC_SOLV_PREC_JACOBI 1
+#define UFC_SOLV_PREC_MG 5  /* geometric multigrid V-cycle, set up by ufc_mg_setup (NM_PREC_AMG = 5,
+                               ufc_core/L2_NM/Solver/LinSolv/NM_Solv_Mgr.f90:35) */
 
 /* Precision of the linear solve. */
 #define UFC_PRECISION_FP64 0        /* FP64 matrix, vectors and dot products      */
@@ -286,6 +288,33 @@ typedef struct {
   int32_t status;                 /* [OUT] */
 } ufc_step_arg;
 
+/* Multigrid preconditioner for a structured box mesh, in the place of the
+ * reference's AMG (NM_AMG_Setup / NM_AMG_V_Cycle / NM_AMG_Smooth / NM_AMG_Galerkin,
+ * ufc_core/L2_NM/Solver/LinSolv/NM_Solv_LinPrecAMG.f90:120-675).  The mesh must be
+ * the nx x ny x nz box numbering: node (i,j,k) = i + (nx+1)(j + (ny+1)k),
+ * element (i,j,k) = i + nx(j + ny k) with nodes in Abaqus order.  Levels halve
+ * the box while nx, ny and nz are even and the level has more than coarse_max
+ * DOF; prolongation is trilinear, coarse operators are Galerkin products
+ * P^T A P formed element by element, Dirichlet DOFs stay eliminated on every
+ * level (a coarse DOF is fixed when its coincident fine DOF is).  Smoother:
+ * Chebyshev polynomial of D^-1 A of the given degree before and after the
+ * coarse correction, on [lambda_max/ratio, 1.1 lambda_max] with lambda_max
+ * from a power iteration; coarsest level: dense inverse (<= 4096 DOF) or a
+ * degree-24 Chebyshev solve.  Uses the assembled FP64 values (and, for J2, the
+ * tangent of the trial state): call it after ufc_elem_compute_ke and again
+ * after every reassembly.  Solve with ufc_solver_algo.precond_type = UFC_SOLV_PREC_MG. */
+typedef struct {
+  int32_t nx, ny, nz;        /* [IN] */
+  int32_t max_levels;        /* [IN] 0: as many as the grid allows */
+  int32_t degree;            /* [IN] Chebyshev degree of each smoothing, 0: 2 */
+  double ratio;              /* [IN] lambda_max / lambda_min of the smoother interval, 0: 15 */
+  int64_t coarse_max;        /* [IN] stop coarsening at or below this many DOF, 0: 1000 */
+  int32_t levels;            /* [OUT] */
+  int32_t reserved;
+  int64_t coarse_dof;        /* [OUT] DOF of the coarsest level */
+  double setup_ms;           /* [OUT] */
+} ufc_mg_arg;
+
 /* Equivalent nodal forces of face loads on C3D8 faces: the 2x2 face Gauss rule
  * of PH_Elem_C3D8_FormFacePressure (ufc_core/L4_PH/Element/Solid3D/PH_Elem_C3D8.f90:2360-2541)
  * and its face numbering (1: nodes 1-2-3-4, zeta = -1; 2: 5-8-7-6, zeta = +1;
@@ -378,6 +407,13 @@ int ufc_pcg_solve(ufc_ctx* ctx, const double* b, double* x, int32_t mem, const u
                   ufc_solver_state* state);
 /* nrhs independent Jacobi-PCG solves sharing every SpMV (one matrix read per
  * iteration for all right-hand sides).  B and X are [nrhs][n_dof]; states[nrhs]. */
+int ufc_mg_setup(ufc_ctx* ctx, ufc_mg_arg* arg);
+/* z = M r: one V-cycle of the multigrid preconditioner ([n_dof] vectors). */
+int ufc_mg_apply(ufc_ctx* ctx, const double* r, double* z, int32_t mem);
+/* Canonical CSR of the operator of multigrid level `level` (0 = the assembled
+ * matrix), as ufc_csr_export; ufc_mg_level_info gives its DOF and non-zeros. */
+int ufc_mg_level_info(ufc_ctx* ctx, int32_t level, int64_t* n_dof, int64_t* nnz);
+int ufc_mg_export(ufc_ctx* ctx, int32_t level, const ufc_csr_export_arg* arg);
 int ufc_pcg_solve_block(ufc_ctx* ctx, int32_t nrhs, const double* B, double* X, int32_t mem,
                         const ufc_solver_algo* algo, ufc_solver_state* states);
 int ufc_last_timing(const ufc_ctx* ctx, ufc_timing_info* info);

@@ -25,7 +25,7 @@ STRUCTS = {
     "ufc_pattern_info": "PatternInfo", "ufc_csr_export_arg": "CsrExportArg", "ufc_elem_ke_arg": "ElemKeArg",
     "ufc_elem_fe_arg": "ElemFeArg", "ufc_mat_update_arg": "MatUpdateArg", "ufc_solver_algo": "SolverAlgo",
     "ufc_solver_state": "SolverState", "ufc_nr_arg": "NrArg", "ufc_timing_info": "TimingInfo",
-    "ufc_step_arg": "StepArg", "ufc_face_load_arg": "FaceLoadArg",
+    "ufc_step_arg": "StepArg", "ufc_face_load_arg": "FaceLoadArg", "ufc_mg_arg": "MgArg",
 }
 
 

@@ -1,0 +1,161 @@
+"""Geometric multigrid preconditioner (ufc_mg_setup) on the GPU: the Galerkin
+coarse operators against P^T A P formed with scipy from the oracle's matrix,
+symmetry and positivity of the V-cycle, and MG-PCG solutions against
+Jacobi-PCG (linear elastic and J2 tangent)."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+pytestmark = pytest.mark.gpu
+
+
+def _prolongation(nxc, nyc, nzc, fixed_f, fixed_c):
+    """Trilinear P from the (nxc, nyc, nzc) box to the box twice as fine, zero
+    at fixed fine rows and fixed coarse columns."""
+    nxf, nyf, nzf = 2 * nxc, 2 * nyc, 2 * nzc
+    rows, cols, vals = [], [], []
+    par = lambda i: [(i // 2, 1.0)] if i % 2 == 0 else [(i // 2, 0.5), (i // 2 + 1, 0.5)]  # noqa: E731
+    for k in range(nzf + 1):
+        for j in range(nyf + 1):
+            for i in range(nxf + 1):
+                f = i + (nxf + 1) * (j + (nyf + 1) * k)
+                for K, wk in par(k):
+                    for J, wj in par(j):
+                        for I, wi in par(i):
+                            c = I + (nxc + 1) * (J + (nyc + 1) * K)
+                            for d in range(3):
+                                if not fixed_f[3 * f + d] and not fixed_c[3 * c + d]:
+                                    rows.append(3 * f + d)
+                                    cols.append(3 * c + d)
+                                    vals.append(wi * wj * wk)
+    nf, nc = 3 * (nxf + 1) * (nyf + 1) * (nzf + 1), 3 * (nxc + 1) * (nyc + 1) * (nzc + 1)
+    return sp.csr_matrix((vals, (rows, cols)), shape=(nf, nc))
+
+
+def _coarse_fixed(fixed_f, nxc, nyc, nzc):
+    nxf, nyf = 2 * nxc, 2 * nyc
+    out = np.zeros(3 * (nxc + 1) * (nyc + 1) * (nzc + 1), dtype=bool)
+    for k in range(nzc + 1):
+        for j in range(nyc + 1):
+            for i in range(nxc + 1):
+                c = i + (nxc + 1) * (j + (nyc + 1) * k)
+                f = 2 * i + (nxf + 1) * (2 * j + (nyf + 1) * 2 * k)
+                out[3 * c:3 * c + 3] = fixed_f[3 * f:3 * f + 3]
+    return out
+
+
+def _dense(rp, col, val, n):
+    return sp.csr_matrix((val, col, rp), shape=(n, n)).toarray()
+
+
+def _eliminated(Am, fixed):
+    A = np.array(Am, dtype=np.float64)
+    A[fixed, :] = 0.0
+    A[:, fixed] = 0.0
+    A[fixed, fixed] = 1.0
+    return A
+
+
+def test_galerkin_coarse_operators(pkg, orc):
+    n = 4
+    E = pkg.mesh.lognormal_moduli(n ** 3, seed=3)
+    p = pkg.mesh.cantilever(n, n, n, float(n), float(n), float(n), E=E)
+    m = pkg.FemModel.from_problem(p)
+    m.assemble(pkg.BUILD_FP64)
+    levels, cdof, _ = m.mg_setup(n, n, n, coarse_max=1)
+    assert levels == 3 and cdof == 3 * 8
+    A0 = orc.Model(p).assemble(eliminate=False)
+    A = sp.csr_matrix((A0.val, A0.col, A0.row_ptr), shape=(p.n_dof, p.n_dof))
+    fixed = np.zeros(p.n_dof, dtype=bool)
+    fixed[p.fixed] = True
+    # level 0 is the assembled matrix
+    rp, col, val = m.mg_export(0)
+    np.testing.assert_allclose(_dense(rp, col, val, p.n_dof), _eliminated(A.toarray(), fixed), rtol=0,
+                               atol=1e-12 * abs(A).max())
+    Af, ff, nc = A, fixed, n
+    for lev in (1, 2):
+        nc //= 2
+        fc = _coarse_fixed(ff, nc, nc, nc)
+        P = _prolongation(nc, nc, nc, ff, fc)
+        Ac = (P.T @ Af @ P).toarray()
+        rp, col, val = m.mg_export(lev)
+        got = _dense(rp, col, val, Ac.shape[0])
+        np.testing.assert_allclose(got, _eliminated(Ac, fc), rtol=0, atol=1e-12 * np.abs(Ac).max())
+        # the pattern of the coarse level is the box pattern
+        rpo, colo = orc.csr_pattern((nc + 1) ** 3, pkg.mesh.box_mesh(nc, nc, nc, 1.0, 1.0, 1.0)[1])
+        assert np.array_equal(rp, rpo) and np.array_equal(col, colo)
+        Af = sp.csr_matrix(Ac)  # the next level multiplies the masked, uneliminated operator
+        ff = fc
+
+
+def test_vcycle_symmetric_positive(pkg):
+    p = pkg.mesh.lognormal_cantilever(8, 4, 4, seed=6)
+    m = pkg.FemModel.from_problem(p)
+    m.assemble(pkg.BUILD_FP64)
+    m.mg_setup(8, 4, 4, coarse_max=30)
+    rng = np.random.default_rng(1)
+    a, b = rng.standard_normal(p.n_dof), rng.standard_normal(p.n_dof)
+    Ma, Mb = m.mg_apply(a), m.mg_apply(b)
+    assert abs(a @ Mb - b @ Ma) <= 1e-11 * abs(a @ Mb)
+    assert a @ Ma > 0 and b @ Mb > 0
+    np.testing.assert_array_equal(m.mg_apply(a), Ma)  # deterministic
+
+
+@pytest.mark.parametrize("name,make,dims", [
+    ("cantilever_40x8x8", lambda mesh: mesh.config1(), (40, 8, 8)),
+    ("lognormal_32x16x16", lambda mesh: mesh.lognormal_cantilever(32, 16, 16, seed=2), (32, 16, 16)),
+])
+def test_mg_pcg_matches_jacobi(pkg, orc, name, make, dims):
+    p = make(pkg.mesh)
+    m = pkg.FemModel.from_problem(p)
+    m.assemble(pkg.BUILD_FP64)
+    levels, cdof, _ = m.mg_setup(*dims)
+    assert levels >= 3
+    b = pkg.lifted_rhs(m, p.f)
+    xj, sj = m.solve(b, pkg.SolverAlgo(tolerance=1e-10))
+    xm, sm = m.solve(b, pkg.SolverAlgo(tolerance=1e-10, precond_type=pkg.SOLV_PREC_MG))
+    assert sm.converged and sm.rnorm <= 1e-10
+    # the residual of the multigrid solution with the oracle's matrix
+    K = orc.Model(p).assemble()
+    assert np.linalg.norm(b - K.matvec(xm)) <= 2e-10 * np.linalg.norm(b)
+    # both solutions meet rtol 1e-10; they agree to the conditioning of K
+    assert np.linalg.norm(xm - xj) <= 1e-6 * np.linalg.norm(xj)
+    assert sm.niter * 8 <= sj.niter, (sm.niter, sj.niter)
+
+
+def test_mg_on_j2_tangent(pkg):
+    p = pkg.mesh.j2_bar(8, 4, 4)
+    m = pkg.FemModel.from_problem(p)
+    for s in (1, 2, 3):
+        assert m.nr_increment(pkg.mesh.j2_bar_target(p, s, n_steps=3, strain=0.006)).converged
+        m.commit()
+    # the tangent of the committed plastic state, and a right-hand side on the free DOFs
+    u = m.displacement()
+    m.internal_force(u, update_state=True)
+    m.assemble(pkg.BUILD_FP64)
+    m.mg_setup(8, 4, 4, coarse_max=30)
+    b = np.random.default_rng(4).standard_normal(p.n_dof)
+    b[p.fixed] = 0.0
+    xj, _ = m.solve(b, pkg.SolverAlgo(tolerance=1e-12))
+    xm, sm = m.solve(b, pkg.SolverAlgo(tolerance=1e-10, precond_type=pkg.SOLV_PREC_MG))
+    assert sm.converged
+    assert np.linalg.norm(xm - xj) <= 1e-8 * np.linalg.norm(xj)
+
+
+def test_mg_errors(pkg):
+    p = pkg.mesh.lognormal_cantilever(8, 4, 4, seed=6)
+    m = pkg.FemModel.from_problem(p)
+    m.assemble(pkg.BUILD_FP64)
+    with pytest.raises(pkg.UfcError) as ei:
+        m.mg_setup(4, 8, 4)  # not this box's numbering
+    assert ei.value.status_code == 1
+    m.mg_setup(8, 4, 4, coarse_max=30)
+    m.assemble(pkg.BUILD_FP64)  # the hierarchy is now stale
+    with pytest.raises(pkg.UfcError) as ei:
+        m.solve(pkg.lifted_rhs(m, p.f), pkg.SolverAlgo(precond_type=pkg.SOLV_PREC_MG))
+    assert ei.value.status_code == 1 and "ufc_mg_setup" in ei.value.message
+    q = pkg.mesh.unit_cube_uniaxial()
+    m1 = pkg.FemModel.from_problem(q)
+    m1.assemble(pkg.BUILD_FP64)
+    with pytest.raises(pkg.UfcError):
+        m1.mg_setup(1, 1, 1)  # cannot be coarsened

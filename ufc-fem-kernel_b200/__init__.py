@@ -29,6 +29,8 @@ REFINE_KEEP_DIRECTION = _abi.REFINE_KEEP_DIRECTION
 REFINE_RESTART = _abi.REFINE_RESTART
 MAT_ELASTIC_ISO = _abi.MAT_ELASTIC_ISO
 MAT_J2_ISO = _abi.MAT_J2_ISO
+SOLV_PREC_JACOBI = _abi.SOLV_PREC_JACOBI
+SOLV_PREC_MG = _abi.SOLV_PREC_MG
 STATUS_OK = _abi.STATUS_OK
 STATUS_INVALID = _abi.STATUS_INVALID
 STATUS_NOT_CONVERGED = _abi.STATUS_NOT_CONVERGED

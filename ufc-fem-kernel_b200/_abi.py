@@ -36,6 +36,7 @@ MAT_J2_ISO = 201
 SOLV_METHOD_CG = 3
 SOLV_PREC_NONE = 0
 SOLV_PREC_JACOBI = 1
+SOLV_PREC_MG = 5
 PRECISION_FP64 = 0
 PRECISION_FP32_REFINE = 1
 PRECISION_FP32_MATRIX = 2
@@ -123,6 +124,12 @@ class StepArg(C.Structure):
                 ("status", _i32)]
 
 
+class MgArg(C.Structure):
+    _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("max_levels", _i32), ("degree", _i32), ("ratio", _d),
+                ("coarse_max", _i64), ("levels", _i32), ("reserved", _i32), ("coarse_dof", _i64),
+                ("setup_ms", _d)]
+
+
 class FaceLoadArg(C.Structure):
     _fields_ = [("n_faces", _i32), ("elem", _p), ("face", _p), ("traction", _p), ("pressure", _p),
                 ("index_base", _i32), ("mem", _i32), ("f", _p)]
@@ -155,6 +162,10 @@ _SIGS = {
     "ufc_last_residual_history": [_p, _p, _i32, C.POINTER(_i32)],
     "ufc_nr_increment": [_p, C.POINTER(NrArg)],
     "ufc_nr_step": [_p, C.POINTER(StepArg)],
+    "ufc_mg_setup": [_p, C.POINTER(MgArg)],
+    "ufc_mg_apply": [_p, _p, _p, _i32],
+    "ufc_mg_level_info": [_p, _i32, C.POINTER(_i64), C.POINTER(_i64)],
+    "ufc_mg_export": [_p, _i32, C.POINTER(CsrExportArg)],
     "ufc_load_faces": [_p, C.POINTER(FaceLoadArg)],
     "ufc_stress_nodal": [_p, _p, _p, _p, _i32],
     "ufc_reactions": [_p, _p, _p, _p, _i32],

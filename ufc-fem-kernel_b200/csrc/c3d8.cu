@@ -516,6 +516,7 @@ int assemble(Ctx* c, int build, double* elapsed_ms) {
                 "ufc_elem_compute_ke: J2 tangent needs ufc_elem_compute_fint(update_state=1) first");
   UFC_TRY(ensure_pairs(c));
   release_graphs(c);  // captured CG batches hold pointers to the values they read
+  mg_mark_stale(c);
   cudaEvent_t e0, e1;
   UFC_CUDA(c, cudaEventCreate(&e0));
   UFC_CUDA(c, cudaEventCreate(&e1));

@@ -129,6 +129,8 @@ int sync(Ctx* c) {
 
 void free_all(Ctx* c) {
   release_graphs(c);
+  mg_free(c);
+  dfree(&c->z64);
   dfree(&c->coords); dfree(&c->conn); dfree(&c->props); dfree(&c->col_elems);
   dfree(&c->brow); dfree(&c->bcol); dfree(&c->slice_ptr); dfree(&c->sell_col); dfree(&c->slot); dfree(&c->dpos);
   dfree(&c->val64); dfree(&c->val32); dfree(&c->dinv64); dfree(&c->dinv32);
@@ -212,7 +214,6 @@ __global__ void k_gather_dofs(int32_t nfix, const int32_t* __restrict__ dofs, co
 
 using namespace ufc;
 
-struct ufc_ctx : public ufc::Ctx {};
 
 #define CTX_CHECK(c)                 \
   do {                               \
@@ -511,6 +512,50 @@ int ufc_stress_eval(ufc_ctx* c, const double* u, double* sig, double* vm, int32_
   UFC_TRY(finish(c, ss));
   UFC_TRY(finish(c, sv));
   return sync(c);
+}
+
+int ufc_mg_setup(ufc_ctx* c, ufc_mg_arg* a) {
+  CTX_CHECK(c);
+  if (!a) return fail(c, UFC_STATUS_INVALID, "ufc_mg_setup: NULL arg");
+  Scope sc(c);
+  a->levels = 0;
+  a->coarse_dof = 0;
+  a->setup_ms = 0.0;
+  UFC_TRY(mg_setup(c, a));
+  return sync(c);
+}
+
+int ufc_mg_apply(ufc_ctx* c, const double* r, double* z, int32_t mem) {
+  CTX_CHECK(c);
+  if (!r || !z) return fail(c, UFC_STATUS_INVALID, "ufc_mg_apply: NULL vector");
+  Scope sc(c);
+  Staged<double> sr, sz;
+  UFC_TRY(stage_in(c, sr, r, c->n, mem));
+  UFC_TRY(stage_out(c, sz, z, c->n, mem));
+  UFC_TRY(mg_apply(c, sr.dev, sz.dev));
+  UFC_TRY(finish(c, sz));
+  return sync(c);
+}
+
+int ufc_mg_level_info(ufc_ctx* c, int32_t level, int64_t* n_dof, int64_t* nnz) {
+  CTX_CHECK(c);
+  Ctx* lc = nullptr;
+  UFC_TRY(mg_level_ctx(c, level, &lc));
+  if (n_dof) *n_dof = lc->n;
+  if (nnz) *nnz = 9 * lc->nnzb;
+  return UFC_STATUS_OK;
+}
+
+int ufc_mg_export(ufc_ctx* c, int32_t level, const ufc_csr_export_arg* a) {
+  CTX_CHECK(c);
+  if (!a) return fail(c, UFC_STATUS_INVALID, "ufc_mg_export: NULL arg");
+  Ctx* lc = nullptr;
+  UFC_TRY(mg_level_ctx(c, level, &lc));
+  Scope sc(c);
+  UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int s = export_csr(lc, a);
+  if (s != UFC_STATUS_OK && lc != c) return fail(c, s, lc->err);
+  return s;
 }
 
 int ufc_load_faces(ufc_ctx* c, const ufc_face_load_arg* a) {

@@ -845,6 +845,24 @@ int64_t spmv_bytes(const Ctx* c, int precision) {
   return c->nnzb * (9 * sv + 4) + 4 * ((int64_t)c->N + 1) + 2 * c->n * sx;
 }
 
+void spmv64_on(const Ctx* lvl, cudaStream_t st, const double* x, double* y) {
+  launch_spmv<double, double, double, kPlain>(lvl, st, lvl->val64, x, y);
+}
+
+void cg_spmv64(Ctx* c, const double* p, double* q) {
+  launch_spmv<double, double, double, kCg>(c, c->stream, c->val64, p, q);
+}
+
+int true_residual_fp64(Ctx* c, bool want_bb) {
+  launch_spmv<double, double, double, kPlain>(c, c->stream, c->val64, c->x64, c->y64);
+  UFC_CUDA(c, cudaGetLastError());
+  k_resid<<<vec_grid(c->n), kVecBlock, 0, c->stream>>>(c->n, c->b64, c->y64, c->y64, c->scal, c->partials,
+                                                       want_bb ? 1 : 0);
+  UFC_CUDA(c, cudaGetLastError());
+  c->launches += 2;
+  return UFC_STATUS_OK;
+}
+
 int spmv(Ctx* c, int precision, const void* x, void* y) {
   if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_spmv: pattern not built");
   const int sg = (int)((c->nslices * kSlice + kSpmvBlock - 1) / kSpmvBlock);
@@ -876,8 +894,9 @@ int spmv(Ctx* c, int precision, const void* x, void* y) {
 int pcg_solve(Ctx* c, const double* b, double* x, const ufc_solver_algo* algo, ufc_solver_state* st) {
   if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: pattern not built");
   if (algo->method != UFC_SOLV_METHOD_CG) return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve: method must be CG");
-  if (algo->precond_type != UFC_SOLV_PREC_JACOBI && algo->precond_type != UFC_SOLV_PREC_NONE)
-    return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve: preconditioner must be Jacobi or none");
+  if (algo->precond_type != UFC_SOLV_PREC_JACOBI && algo->precond_type != UFC_SOLV_PREC_NONE &&
+      algo->precond_type != UFC_SOLV_PREC_MG)
+    return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve: preconditioner must be Jacobi, multigrid or none");
   const int prec = algo->precision_mode;
   if (prec == UFC_PRECISION_FP64 && !c->has_val64)
     return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: FP64 values not assembled (UFC_BUILD_FP64)");
@@ -898,6 +917,16 @@ int pcg_solve(Ctx* c, const double* b, double* x, const ufc_solver_algo* algo, u
   else
     UFC_CUDA(c, cudaMemsetAsync(c->x64, 0, sizeof(double) * c->n, c->stream));
   int s;
+  if (algo->precond_type == UFC_SOLV_PREC_MG) {
+    if (prec != UFC_PRECISION_FP64)
+      return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve: the multigrid preconditioner runs in FP64");
+    s = pcg_mg(c, algo, st);
+    if (s != UFC_STATUS_OK && s != UFC_STATUS_NOT_CONVERGED) return s;
+    st->fp64_iters = 0;
+    UFC_CUDA(c, cudaMemcpyAsync(x, c->x64, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream));
+    if (s == UFC_STATUS_NOT_CONVERGED) fail(c, UFC_STATUS_NOT_CONVERGED, "[NM_Solver_PCG]: did not converge");
+    return s;
+  }
   if (prec == UFC_PRECISION_FP64)
     s = pcg_run<double, double, double>(c, algo, st);
   else if (prec == UFC_PRECISION_FP32_MATRIX)

@@ -48,6 +48,8 @@ enum DevErr : int32_t {
   kDevPattern = 16,
 };
 
+struct Mg;  // multigrid hierarchy (mg.cu)
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;  // own non-blocking stream: all work runs here
@@ -139,6 +141,10 @@ struct Ctx {
   double* Dt = nullptr;     // [G*36] consistent tangent of the trial state
   bool has_trial = false;
 
+  // multigrid preconditioner (ufc_mg_setup), and the preconditioned vector z
+  Mg* mg = nullptr;
+  double* z64 = nullptr;
+
   // cached CUDA graphs of CG batches
   cudaGraphExec_t cg_graph[kGraphSlots] = {};
   int cg_graph_batch[kGraphSlots] = {};
@@ -169,6 +175,18 @@ int mat_update_batch(Ctx* c, const ufc_mat_update_arg* a, const double* props, c
                      int32_t* yielded);
 int stress_eval(Ctx* c, const double* u, double* sig, double* vm);
 int adjoint_sens(Ctx* c, int nrhs, const double* U, const double* L, double* g);
+
+// mg.cu
+int mg_setup(Ctx* c, ufc_mg_arg* a);
+void mg_free(Ctx* c);
+void mg_mark_stale(Ctx* c);  // the matrix changed: the hierarchy must be set up again
+int mg_apply(Ctx* c, const double* r, double* z);
+int mg_level_ctx(Ctx* c, int32_t level, Ctx** out);
+int pcg_mg(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st);
+// FP64 SELL SpMV (full storage) of any context's values, on the given stream (solver.cu)
+void spmv64_on(const Ctx* lvl, cudaStream_t st, const double* x, double* y);
+void cg_spmv64(Ctx* c, const double* p, double* q);  // q = K p, p.q and alpha = r.z / p.q into the scalars
+int true_residual_fp64(Ctx* c, bool want_bb);  // y64 = b64 - K x64, scal->true_rr (and bb)
 
 // output.cu
 int face_loads(Ctx* c, int32_t n_faces, const int32_t* h_elem, const int32_t* h_face, const double* traction,
@@ -210,6 +228,9 @@ void dfree(T** p) {
 }
 
 }  // namespace ufc
+
+// the C-ABI's opaque context is the internal one
+struct ufc_ctx : public ufc::Ctx {};
 
 #define UFC_TRY(expr)                      \
   do {                                     \

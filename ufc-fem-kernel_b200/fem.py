@@ -342,6 +342,35 @@ class FemModel:
             self._check(st, "ufc_pcg_solve_block")
         return X, [SolverState.from_c(s, st) for s in cs]
 
+    # ---------------------------------------------------------------- multigrid
+    def mg_setup(self, nx, ny, nz, max_levels=0, degree=0, ratio=0.0, coarse_max=0):
+        """Geometric multigrid hierarchy of the nx x ny x nz box (ufc_mg_setup);
+        solve with SolverAlgo(precond_type=SOLV_PREC_MG).  Returns
+        (levels, coarsest DOF, set-up ms)."""
+        a = A.MgArg()
+        a.nx, a.ny, a.nz, a.max_levels, a.degree = int(nx), int(ny), int(nz), int(max_levels), int(degree)
+        a.ratio, a.coarse_max = float(ratio), int(coarse_max)
+        self._check(self.lib.ufc_mg_setup(self.h, C.byref(a)), "ufc_mg_setup")
+        return a.levels, a.coarse_dof, a.setup_ms
+
+    def mg_apply(self, r, out=None):
+        """z = M r, one V-cycle."""
+        z = out if out is not None else self._empty(self.n_dof, np.float64, r)
+        rb, zb = _Buf(r, np.float64, self.n_dof), _Buf(z, np.float64, self.n_dof, writable=True)
+        self._check(self.lib.ufc_mg_apply(self.h, rb.ptr, zb.ptr, _same_mem(rb, zb)), "ufc_mg_apply")
+        return z
+
+    def mg_export(self, level):
+        """Canonical CSR (row_ptr, col, values) of the operator of one multigrid level."""
+        n, nnz = C.c_int64(0), C.c_int64(0)
+        self._check(self.lib.ufc_mg_level_info(self.h, int(level), C.byref(n), C.byref(nnz)), "ufc_mg_level_info")
+        rp = np.zeros(n.value + 1, dtype=np.int64)
+        col = np.zeros(nnz.value, dtype=np.int32)
+        v = np.zeros(nnz.value)
+        a = A.CsrExportArg(0, A.MEM_HOST, rp.ctypes.data, col.ctypes.data, v.ctypes.data, None)
+        self._check(self.lib.ufc_mg_export(self.h, int(level), C.byref(a)), "ufc_mg_export")
+        return rp, col, v
+
     def set_instrument(self, on=True):
         self._check(self.lib.ufc_ctx_set_instrument(self.h, int(on)), "ufc_ctx_set_instrument")
 
