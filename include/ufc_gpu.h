@@ -301,16 +301,21 @@ typedef struct {
  * coarse correction, on [lambda_max/ratio, 1.1 lambda_max] with lambda_max
  * from a power iteration; coarsest level: dense inverse (<= 4096 DOF) or a
  * degree-24 Chebyshev solve.  Uses the assembled FP64 values (and, for J2, the
- * tangent of the trial state): call it after ufc_elem_compute_ke and again
- * after every reassembly.  Solve with ufc_solver_algo.precond_type = UFC_SOLV_PREC_MG. */
+ * tangent of the trial state): call it after ufc_elem_compute_ke; after a
+ * reassembly the numerical part (coarse operators, smoother bounds, coarsest
+ * inverse) is rebuilt on the boxes already set up, at the next multigrid solve.
+ * Solve with ufc_solver_algo.precond_type = UFC_SOLV_PREC_MG and precision FP64
+ * (the outer PCG; the cycle's own precision is chosen here). */
 typedef struct {
   int32_t nx, ny, nz;        /* [IN] */
   int32_t max_levels;        /* [IN] 0: as many as the grid allows */
   int32_t degree;            /* [IN] Chebyshev degree of each smoothing, 0: 2 */
   double ratio;              /* [IN] lambda_max / lambda_min of the smoother interval, 0: 15 */
-  int64_t coarse_max;        /* [IN] stop coarsening at or below this many DOF, 0: 1000 */
+  int64_t coarse_max;        /* [IN] stop coarsening at or below this many DOF, 0: 300 */
   int32_t levels;            /* [OUT] */
-  int32_t reserved;
+  int32_t precision;         /* [IN] UFC_PRECISION_FP64: FP64 cycle; UFC_PRECISION_FP32_REFINE: the
+                                cycle in FP32 on values rounded from the FP64 operators (the PCG
+                                around it stays FP64) */
   int64_t coarse_dof;        /* [OUT] DOF of the coarsest level */
   double setup_ms;           /* [OUT] */
 } ufc_mg_arg;

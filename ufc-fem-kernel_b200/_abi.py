@@ -126,7 +126,7 @@ class StepArg(C.Structure):
 
 class MgArg(C.Structure):
     _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("max_levels", _i32), ("degree", _i32), ("ratio", _d),
-                ("coarse_max", _i64), ("levels", _i32), ("reserved", _i32), ("coarse_dof", _i64),
+                ("coarse_max", _i64), ("levels", _i32), ("precision", _i32), ("coarse_dof", _i64),
                 ("setup_ms", _d)]
 
 

@@ -25,6 +25,11 @@
 // atomics and are deterministic; the coarse matrices are assembled colour by
 // colour like the fine one.
 //
+// Precision: the cycle runs in FP64, or (precision = UFC_PRECISION_FP32_REFINE)
+// in FP32 on values rounded from the FP64 operators, half the bytes; the PCG
+// around it stays FP64 (matrix, vectors, residual), so the preconditioner's
+// rounding changes only the iteration count, never the answer.
+//
 // The PCG is NM_Solver_PCG's recurrence with z = M r from the V-cycle; all of
 // an iteration's kernels (SpMV, updates, the cycle on every level) are
 // captured once into a CUDA graph and replayed.
@@ -46,10 +51,15 @@ struct MgLevel {
   ufc_ctx* own = nullptr;    // levels >= 1: a context holding the coarse box
   int32_t nx = 0, ny = 0, nz = 0;
   double* ke = nullptr;      // levels >= 1: Galerkin element matrices [E][24][24]
+  // FP64 cycle: level vectors (level 0: x and b are the PCG's z and r)
   double *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *w = nullptr;
-  bool own_xb = false;       // x and b allocated here (not the PCG's r and z)
+  // FP32 cycle: level vectors, and the level's values and diagonal rounded to FP32
+  float *x32 = nullptr, *b32 = nullptr, *r32 = nullptr, *d32 = nullptr, *w32 = nullptr;
+  float *val32 = nullptr, *dinv32 = nullptr;
+  bool own_xb = false;       // x and b allocated here
   double lmax = 0.0;
   double* inv = nullptr;     // coarsest level: dense inverse [n][n]
+  float* inv32 = nullptr;
 };
 
 struct Mg {
@@ -57,6 +67,7 @@ struct Mg {
   int degree = 2;
   double ratio = 15.0;
   bool stale = false;
+  bool fp32 = false;         // the cycle runs in FP32 (values, vectors); the PCG around it in FP64
   int cheb_coarse = 0;       // degree of the coarsest Chebyshev solve (0: dense inverse)
 };
 
@@ -234,16 +245,17 @@ __global__ void k_mg_dinv(int32_t N, const int32_t* __restrict__ dpos, const dou
 
 // r_c = P^T r_f: one thread per coarse node gathers the fine nodes within one
 // fine spacing of it, weight prod_d (1 or 1/2).
-__global__ void k_mg_restrict(int32_t nxc, int32_t nyc, int32_t nzc, const double* __restrict__ rf,
+template <typename T>
+__global__ void k_mg_restrict(int32_t nxc, int32_t nyc, int32_t nzc, const T* __restrict__ rf,
                               const uint8_t* __restrict__ fixed_f, const uint8_t* __restrict__ fixed_c,
-                              double* __restrict__ rc, const CgScalars* __restrict__ scal) {
+                              T* __restrict__ rc, const CgScalars* __restrict__ scal) {
   if (scal && scal->stop) return;
   const int64_t nc = (int64_t)(nxc + 1) * (nyc + 1) * (nzc + 1);
   const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nc) return;
   const int nxf = 2 * nxc, nyf = 2 * nyc, nzf = 2 * nzc;
   const int64_t I = v % (nxc + 1), J = (v / (nxc + 1)) % (nyc + 1), K = v / ((int64_t)(nxc + 1) * (nyc + 1));
-  double s[3] = {0.0, 0.0, 0.0};
+  T s[3] = {T(0), T(0), T(0)};
   for (int dk = -1; dk <= 1; ++dk) {
     const int64_t k = 2 * K + dk;
     if (k < 0 || k > nzf) continue;
@@ -253,7 +265,7 @@ __global__ void k_mg_restrict(int32_t nxc, int32_t nyc, int32_t nzc, const doubl
       for (int di = -1; di <= 1; ++di) {
         const int64_t i = 2 * I + di;
         if (i < 0 || i > nxf) continue;
-        const double w = (di ? 0.5 : 1.0) * (dj ? 0.5 : 1.0) * (dk ? 0.5 : 1.0);
+        const T w = T((di ? 0.5 : 1.0) * (dj ? 0.5 : 1.0) * (dk ? 0.5 : 1.0));
         const int64_t f = box_node(i, j, k, nxf, nyf);
 #pragma unroll
         for (int d = 0; d < 3; ++d)
@@ -262,13 +274,14 @@ __global__ void k_mg_restrict(int32_t nxc, int32_t nyc, int32_t nzc, const doubl
     }
   }
 #pragma unroll
-  for (int d = 0; d < 3; ++d) rc[3 * v + d] = fixed_c[3 * v + d] ? 0.0 : s[d];
+  for (int d = 0; d < 3; ++d) rc[3 * v + d] = fixed_c[3 * v + d] ? T(0) : s[d];
 }
 
 // x_f += P x_c: one thread per fine node gathers its 1, 2, 4 or 8 coarse parents.
-__global__ void k_mg_prolong_add(int32_t nxc, int32_t nyc, int32_t nzc, const double* __restrict__ xc,
+template <typename T>
+__global__ void k_mg_prolong_add(int32_t nxc, int32_t nyc, int32_t nzc, const T* __restrict__ xc,
                                  const uint8_t* __restrict__ fixed_f, const uint8_t* __restrict__ fixed_c,
-                                 double* __restrict__ xf, const CgScalars* __restrict__ scal) {
+                                 T* __restrict__ xf, const CgScalars* __restrict__ scal) {
   if (scal && scal->stop) return;
   const int nxf = 2 * nxc, nyf = 2 * nyc, nzf = 2 * nzc;
   const int64_t nf = (int64_t)(nxf + 1) * (nyf + 1) * (nzf + 1);
@@ -277,8 +290,8 @@ __global__ void k_mg_prolong_add(int32_t nxc, int32_t nyc, int32_t nzc, const do
   const int64_t i = v % (nxf + 1), j = (v / (nxf + 1)) % (nyf + 1), k = v / ((int64_t)(nxf + 1) * (nyf + 1));
   const int64_t i0 = i >> 1, j0 = j >> 1, k0 = k >> 1;
   const int ni = (i & 1) ? 2 : 1, nj = (j & 1) ? 2 : 1, nk = (k & 1) ? 2 : 1;
-  const double w = (ni == 2 ? 0.5 : 1.0) * (nj == 2 ? 0.5 : 1.0) * (nk == 2 ? 0.5 : 1.0);
-  double s[3] = {0.0, 0.0, 0.0};
+  const T w = T((ni == 2 ? 0.5 : 1.0) * (nj == 2 ? 0.5 : 1.0) * (nk == 2 ? 0.5 : 1.0));
+  T s[3] = {T(0), T(0), T(0)};
   for (int c = 0; c < nk; ++c)
     for (int b = 0; b < nj; ++b)
       for (int a = 0; a < ni; ++a) {
@@ -296,13 +309,14 @@ __global__ void k_mg_prolong_add(int32_t nxc, int32_t nyc, int32_t nzc, const do
 // Sparse Linear Systems, Alg. 12.1, with the Jacobi preconditioner).
 // Start: r = b - w (w = A x, or zero when x starts at zero), d = D^-1 r / theta,
 // x (+)= d.
-__global__ void k_cheb_start(int64_t n, const double* __restrict__ b, const double* __restrict__ w,
-                             const double* __restrict__ dinv, double inv_theta, int x_zero, double* __restrict__ x,
-                             double* __restrict__ r, double* __restrict__ d, const CgScalars* __restrict__ scal) {
+template <typename T>
+__global__ void k_cheb_start(int64_t n, const T* __restrict__ b, const T* __restrict__ w,
+                             const T* __restrict__ dinv, T inv_theta, int x_zero, T* __restrict__ x,
+                             T* __restrict__ r, T* __restrict__ d, const CgScalars* __restrict__ scal) {
   if (scal && scal->stop) return;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double ri = b[i] - (x_zero ? 0.0 : w[i]);
-    const double di = dinv[i] * ri * inv_theta;
+    const T ri = b[i] - (x_zero ? T(0) : w[i]);
+    const T di = dinv[i] * ri * inv_theta;
     r[i] = ri;
     d[i] = di;
     x[i] = x_zero ? di : x[i] + di;
@@ -310,13 +324,14 @@ __global__ void k_cheb_start(int64_t n, const double* __restrict__ b, const doub
 }
 
 // Step: r -= w (w = A d), d = c1 d + c2 D^-1 r, x += d.
-__global__ void k_cheb_step(int64_t n, const double* __restrict__ w, const double* __restrict__ dinv, double c1,
-                            double c2, double* __restrict__ x, double* __restrict__ r, double* __restrict__ d,
+template <typename T>
+__global__ void k_cheb_step(int64_t n, const T* __restrict__ w, const T* __restrict__ dinv, T c1, T c2,
+                            T* __restrict__ x, T* __restrict__ r, T* __restrict__ d,
                             const CgScalars* __restrict__ scal) {
   if (scal && scal->stop) return;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double ri = r[i] - w[i];
-    const double di = c1 * d[i] + c2 * dinv[i] * ri;
+    const T ri = r[i] - w[i];
+    const T di = c1 * d[i] + c2 * dinv[i] * ri;
     r[i] = ri;
     d[i] = di;
     x[i] += di;
@@ -324,25 +339,34 @@ __global__ void k_cheb_step(int64_t n, const double* __restrict__ w, const doubl
 }
 
 // out = b - w
-__global__ void k_mg_sub(int64_t n, const double* __restrict__ b, const double* __restrict__ w,
-                         double* __restrict__ out, const CgScalars* __restrict__ scal) {
+template <typename T>
+__global__ void k_mg_sub(int64_t n, const T* __restrict__ b, const T* __restrict__ w, T* __restrict__ out,
+                         const CgScalars* __restrict__ scal) {
   if (scal && scal->stop) return;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = b[i] - w[i];
 }
 
 // x = Inv b (dense, coarsest level), one warp per row.
-__global__ void k_mg_dense(int64_t n, const double* __restrict__ inv, const double* __restrict__ b,
-                           double* __restrict__ x, const CgScalars* __restrict__ scal) {
+template <typename T>
+__global__ void k_mg_dense(int64_t n, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x,
+                           const CgScalars* __restrict__ scal) {
   if (scal && scal->stop) return;
   const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
-  double s = 0.0;
+  T s = T(0);
   for (int64_t j = lane; j < n; j += 32) s += inv[row * n + j] * b[j];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if (lane == 0) x[row] = s;
+}
+
+template <typename A, typename B>
+__global__ void k_mg_convert(int64_t n, const A* __restrict__ a, B* __restrict__ b, const CgScalars* __restrict__ scal) {
+  if (scal && scal->stop) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (B)a[i];
 }
 
 // ||v||^2 into *out (power iteration at set-up).
@@ -428,37 +452,51 @@ int dinv_of(Ctx* lc) {
   return UFC_STATUS_OK;
 }
 
-// lambda_max of D^-1 A on level lv by power iteration (deterministic start).
+__global__ void k_mg_round(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+// lambda_max of D^-1 A on level L by power iteration (deterministic start), in FP64.
 int estimate_lmax(Ctx* owner, MgLevel& L, int iters) {
   Ctx* lc = L.c;
   const int64_t n = lc->n;
   const int g = grid_n(n);
-  k_mg_start_vector<<<g, kBlk, 0, owner->stream>>>(n, lc->fixed, L.d);
-  double* dnorm = nullptr;
-  UFC_CUDA(owner, cudaMalloc((void**)&dnorm, sizeof(double)));
+  double *v = nullptr, *w = nullptr, *dnorm = nullptr;
+  auto cleanup = [&]() {
+    dfree(&v);
+    dfree(&w);
+    dfree(&dnorm);
+  };
+  if (dalloc(owner, &v, n) != UFC_STATUS_OK || dalloc(owner, &w, n) != UFC_STATUS_OK ||
+      dalloc(owner, &dnorm, 1) != UFC_STATUS_OK) {
+    cleanup();
+    return UFC_STATUS_MEM_ERROR;
+  }
+  k_mg_start_vector<<<g, kBlk, 0, owner->stream>>>(n, lc->fixed, v);
   double lam = 0.0, nrm = 0.0;
-  k_mg_norm2<<<g, kBlk, 0, owner->stream>>>(n, L.d, owner->partials, &owner->scal->ticket[6], dnorm);
-  UFC_CUDA(owner, cudaMemcpyAsync(&nrm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, owner->stream));
-  UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
+  k_mg_norm2<<<g, kBlk, 0, owner->stream>>>(n, v, owner->partials, &owner->scal->ticket[6], dnorm);
+  cudaMemcpyAsync(&nrm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, owner->stream);
+  cudaStreamSynchronize(owner->stream);
   nrm = std::sqrt(nrm);
   for (int it = 0; it < iters && nrm > 0.0; ++it) {
-    spmv64_on(lc, owner->stream, L.d, L.w);
-    k_mg_scale_dinv<<<g, kBlk, 0, owner->stream>>>(n, L.w, lc->dinv64, 1.0 / nrm, L.d);
-    k_mg_norm2<<<g, kBlk, 0, owner->stream>>>(n, L.d, owner->partials, &owner->scal->ticket[6], dnorm);
-    double v = 0.0;
-    UFC_CUDA(owner, cudaMemcpyAsync(&v, dnorm, sizeof(double), cudaMemcpyDeviceToHost, owner->stream));
-    UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
-    lam = std::sqrt(v);  // ||D^-1 A v|| / ||v|| with the previous v normalised
+    spmv64_on(lc, owner->stream, v, w);
+    k_mg_scale_dinv<<<g, kBlk, 0, owner->stream>>>(n, w, lc->dinv64, 1.0 / nrm, v);
+    k_mg_norm2<<<g, kBlk, 0, owner->stream>>>(n, v, owner->partials, &owner->scal->ticket[6], dnorm);
+    double q = 0.0;
+    cudaMemcpyAsync(&q, dnorm, sizeof(double), cudaMemcpyDeviceToHost, owner->stream);
+    cudaStreamSynchronize(owner->stream);
+    lam = std::sqrt(q);  // ||D^-1 A v|| / ||v|| with the previous v normalised
     nrm = lam;
   }
-  cudaFree(dnorm);
+  cleanup();
   UFC_CUDA(owner, cudaGetLastError());
   L.lmax = lam;
   return UFC_STATUS_OK;
 }
 
 // Dense inverse of the coarsest matrix (Gauss-Jordan with partial pivoting).
-int dense_inverse(Ctx* owner, MgLevel& L) {
+int dense_inverse(Ctx* owner, MgLevel& L, bool fp32) {
   Ctx* lc = L.c;
   const int64_t n = lc->n, nnz = 9 * lc->nnzb;
   std::vector<int64_t> rp(n + 1);
@@ -502,9 +540,16 @@ int dense_inverse(Ctx* owner, MgLevel& L) {
       }
     }
   }
-  UFC_TRY(dalloc(owner, &L.inv, n * n));
-  UFC_CUDA(owner, cudaMemcpyAsync(L.inv, Inv.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice, owner->stream));
-  UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
+  if (fp32) {
+    std::vector<float> f(Inv.begin(), Inv.end());
+    UFC_TRY(dalloc(owner, &L.inv32, n * n));
+    UFC_CUDA(owner, cudaMemcpyAsync(L.inv32, f.data(), sizeof(float) * n * n, cudaMemcpyHostToDevice, owner->stream));
+    UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
+  } else {
+    UFC_TRY(dalloc(owner, &L.inv, n * n));
+    UFC_CUDA(owner, cudaMemcpyAsync(L.inv, Inv.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice, owner->stream));
+    UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
+  }
   return UFC_STATUS_OK;
 }
 
@@ -513,7 +558,15 @@ void free_level(MgLevel& L) {
   dfree(&L.r);
   dfree(&L.d);
   dfree(&L.w);
+  dfree(&L.r32);
+  dfree(&L.d32);
+  dfree(&L.w32);
+  dfree(&L.x32);
+  dfree(&L.b32);
+  dfree(&L.val32);
+  dfree(&L.dinv32);
   dfree(&L.inv);
+  dfree(&L.inv32);
   if (L.own_xb) {
     dfree(&L.x);
     dfree(&L.b);
@@ -522,51 +575,91 @@ void free_level(MgLevel& L) {
   L.own = nullptr;
 }
 
+// The vectors, values and diagonal of a level in the cycle's precision.
+template <typename T>
+struct View {
+  T *x, *b, *r, *d, *w;
+  const T *val, *dinv, *inv;
+};
+
+View<double> view(MgLevel& L, double*) { return {L.x, L.b, L.r, L.d, L.w, L.c->val64, L.c->dinv64, L.inv}; }
+View<float> view(MgLevel& L, float*) { return {L.x32, L.b32, L.r32, L.d32, L.w32, L.val32, L.dinv32, L.inv32}; }
+
+void spmv_lv(const Ctx* lc, cudaStream_t st, const double* val, const double* x, double* y) {
+  (void)val;
+  spmv64_on(lc, st, x, y);
+}
+void spmv_lv(const Ctx* lc, cudaStream_t st, const float* val, const float* x, float* y) {
+  spmv32_on(lc, st, val, x, y);
+}
+
 // Chebyshev smoothing of A x = b on level L (m steps).
+template <typename T>
 void cheb(Ctx* owner, MgLevel& L, int m, double ratio, bool x_zero, const CgScalars* scal) {
   Ctx* lc = L.c;
+  const View<T> V = view(L, (T*)nullptr);
   const int64_t n = lc->n;
   const int g = grid_n(n);
   const double lmax = 1.1 * L.lmax, lmin = lmax / ratio;
   const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
   const double sigma = theta / delta;
-  if (!x_zero) spmv64_on(lc, owner->stream, L.x, L.w);
-  k_cheb_start<<<g, kBlk, 0, owner->stream>>>(n, L.b, L.w, lc->dinv64, 1.0 / theta, x_zero ? 1 : 0, L.x, L.r, L.d,
-                                              scal);
+  if (!x_zero) spmv_lv(lc, owner->stream, V.val, V.x, V.w);
+  k_cheb_start<T><<<g, kBlk, 0, owner->stream>>>(n, V.b, V.w, V.dinv, (T)(1.0 / theta), x_zero ? 1 : 0, V.x, V.r,
+                                                 V.d, scal);
   double rho = 1.0 / sigma;
   for (int k = 1; k < m; ++k) {
-    spmv64_on(lc, owner->stream, L.d, L.w);
+    spmv_lv(lc, owner->stream, V.val, V.d, V.w);
     const double rho_new = 1.0 / (2.0 * sigma - rho);
-    k_cheb_step<<<g, kBlk, 0, owner->stream>>>(n, L.w, lc->dinv64, rho_new * rho, 2.0 * rho_new / delta, L.x, L.r,
-                                               L.d, scal);
+    k_cheb_step<T><<<g, kBlk, 0, owner->stream>>>(n, V.w, V.dinv, (T)(rho_new * rho), (T)(2.0 * rho_new / delta),
+                                                  V.x, V.r, V.d, scal);
     rho = rho_new;
   }
   owner->launches += 2 * m - (x_zero ? 1 : 0);
 }
 
-// One V-cycle from level l: L.x ~ A_l^-1 L.b.
+// One V-cycle from level l: x ~ A_l^-1 b.
+template <typename T>
 void vcycle(Ctx* owner, Mg& mg, size_t l, const CgScalars* scal) {
   MgLevel& L = mg.lv[l];
   Ctx* lc = L.c;
+  const View<T> V = view(L, (T*)nullptr);
   if (l + 1 == mg.lv.size()) {
-    if (L.inv) {
-      k_mg_dense<<<(int)((lc->n * 32 + kBlk - 1) / kBlk), kBlk, 0, owner->stream>>>(lc->n, L.inv, L.b, L.x, scal);
+    if (V.inv) {
+      k_mg_dense<T><<<(int)((lc->n * 32 + kBlk - 1) / kBlk), kBlk, 0, owner->stream>>>(lc->n, V.inv, V.b, V.x, scal);
       owner->launches += 1;
     } else {
-      cheb(owner, L, mg.cheb_coarse, 1000.0, true, scal);
+      cheb<T>(owner, L, mg.cheb_coarse, 1000.0, true, scal);
     }
     return;
   }
   MgLevel& C = mg.lv[l + 1];
-  cheb(owner, L, mg.degree, mg.ratio, true, scal);
-  spmv64_on(lc, owner->stream, L.x, L.w);
-  k_mg_sub<<<grid_n(lc->n), kBlk, 0, owner->stream>>>(lc->n, L.b, L.w, L.r, scal);
-  k_mg_restrict<<<grid_for(C.c->N, kBlk), kBlk, 0, owner->stream>>>(C.nx, C.ny, C.nz, L.r, lc->fixed, C.c->fixed, C.b, scal);
-  vcycle(owner, mg, l + 1, scal);
-  k_mg_prolong_add<<<grid_for(lc->N, kBlk), kBlk, 0, owner->stream>>>(C.nx, C.ny, C.nz, C.x, lc->fixed, C.c->fixed, L.x,
-                                                              scal);
-  cheb(owner, L, mg.degree, mg.ratio, false, scal);
+  const View<T> W = view(C, (T*)nullptr);
+  cheb<T>(owner, L, mg.degree, mg.ratio, true, scal);
+  spmv_lv(lc, owner->stream, V.val, V.x, V.w);
+  k_mg_sub<T><<<grid_n(lc->n), kBlk, 0, owner->stream>>>(lc->n, V.b, V.w, V.r, scal);
+  k_mg_restrict<T><<<grid_for(C.c->N, kBlk), kBlk, 0, owner->stream>>>(C.nx, C.ny, C.nz, V.r, lc->fixed, C.c->fixed,
+                                                                      W.b, scal);
+  vcycle<T>(owner, mg, l + 1, scal);
+  k_mg_prolong_add<T><<<grid_for(lc->N, kBlk), kBlk, 0, owner->stream>>>(C.nx, C.ny, C.nz, W.x, lc->fixed,
+                                                                        C.c->fixed, V.x, scal);
+  cheb<T>(owner, L, mg.degree, mg.ratio, false, scal);
   owner->launches += 5;
+}
+
+// z = M r on the owner's stream (r, z: FP64 vectors of level 0).
+void run_cycle(Ctx* c, Mg& mg, const double* r, double* z, const CgScalars* scal) {
+  MgLevel& L0 = mg.lv[0];
+  const int64_t n = c->n;
+  if (mg.fp32) {
+    k_mg_convert<double, float><<<grid_n(n), kBlk, 0, c->stream>>>(n, r, L0.b32, scal);
+    vcycle<float>(c, mg, 0, scal);
+    k_mg_convert<float, double><<<grid_n(n), kBlk, 0, c->stream>>>(n, L0.x32, z, scal);
+    c->launches += 2;
+  } else {
+    L0.b = const_cast<double*>(r);
+    L0.x = z;
+    vcycle<double>(c, mg, 0, scal);
+  }
 }
 
 }  // namespace
@@ -580,6 +673,98 @@ void mg_free(Ctx* c) {
   for (auto& L : c->mg->lv) free_level(L);
   delete c->mg;
   c->mg = nullptr;
+}
+
+// The numerical part of the hierarchy, from the owner's current FP64 values
+// (and J2 tangent): Galerkin element matrices, coarse matrices, diagonals,
+// FP32 copies, smoother bounds and the coarsest inverse.  Run at set-up and
+// again, on the same boxes and patterns, whenever the owner reassembles.
+static int mg_alloc(Ctx* c, double** p, int64_t n) { return *p ? UFC_STATUS_OK : dalloc(c, p, n); }
+static int mg_alloc(Ctx* c, float** p, int64_t n) { return *p ? UFC_STATUS_OK : dalloc(c, p, n); }
+
+int mg_refresh(Ctx* c);
+
+int mg_numeric(Ctx* c) {
+  Mg& mg = *c->mg;
+  const bool tangent = c->mat_model == UFC_MAT_J2_ISO;
+  if (tangent && !c->Dt) return fail(c, UFC_STATUS_INVALID, "ufc_mg_setup: no J2 tangent");
+  if (!c->dinv64) return fail(c, UFC_STATUS_INVALID, "ufc_mg_setup: no FP64 diagonal");
+  for (size_t l = 1; l < mg.lv.size(); ++l) {
+    MgLevel& F = mg.lv[l - 1];
+    MgLevel& L = mg.lv[l];
+    Ctx* lc = L.c;
+    UFC_TRY(mg_alloc(c, &L.ke, (int64_t)lc->E * 576));
+    const int grid = lc->E;
+    if (l == 1) {
+      if (tangent)
+        k_mg_galerkin<false, true><<<grid, 64, 0, c->stream>>>(L.nx, L.ny, L.nz, c->coords, c->conn, c->props,
+                                                               c->nprops, c->Dt, nullptr, c->fixed, lc->conn,
+                                                               lc->fixed, L.ke, c->dev_err);
+      else
+        k_mg_galerkin<false, false><<<grid, 64, 0, c->stream>>>(L.nx, L.ny, L.nz, c->coords, c->conn, c->props,
+                                                                c->nprops, nullptr, nullptr, c->fixed, lc->conn,
+                                                                lc->fixed, L.ke, c->dev_err);
+    } else {
+      k_mg_galerkin<true, false><<<grid, 64, 0, c->stream>>>(L.nx, L.ny, L.nz, nullptr, F.c->conn, nullptr, 0,
+                                                             nullptr, F.ke, F.c->fixed, lc->conn, lc->fixed, L.ke,
+                                                             c->dev_err);
+    }
+    UFC_CUDA(c, cudaGetLastError());
+    const int64_t nv = lc->sell_blocks * 9;
+    UFC_TRY(mg_alloc(c, &lc->val64, nv));
+    UFC_TRY(dinv_of(lc));
+    UFC_CUDA(c, cudaMemsetAsync(lc->val64, 0, sizeof(double) * nv, c->stream));
+    for (int col = 0; col < lc->ncol; ++col) {
+      const int32_t ne = lc->col_off[col + 1] - lc->col_off[col];
+      if (ne == 0) continue;
+      k_mg_scatter<<<(int)(((int64_t)ne * 64 + kBlk - 1) / kBlk), kBlk, 0, c->stream>>>(
+          lc->col_elems + lc->col_off[col], ne, lc->conn, L.ke, lc->slot, lc->fixed, lc->val64);
+    }
+    if (lc->nfix > 0)
+      k_mg_fix_diag<<<grid_for(lc->nfix, kBlk), kBlk, 0, c->stream>>>(lc->nfix, lc->fix_dofs, lc->dpos, lc->val64);
+    k_mg_dinv<<<grid_for(lc->n, kBlk), kBlk, 0, c->stream>>>(lc->N, lc->dpos, lc->val64, lc->dinv64);
+    UFC_CUDA(c, cudaGetLastError());
+    lc->has_val64 = true;
+  }
+  UFC_TRY(check_dev_err(c, "ufc_mg_setup"));
+  // level vectors (and FP32 values) in the cycle's precision, smoother bounds, coarsest solve
+  for (size_t l = 0; l < mg.lv.size(); ++l) {
+    MgLevel& L = mg.lv[l];
+    const int64_t n = L.c->n;
+    if (mg.fp32) {
+      const int64_t nv = L.c->sell_blocks * 9;
+      UFC_TRY(mg_alloc(c, &L.r32, n));
+      UFC_TRY(mg_alloc(c, &L.d32, n));
+      UFC_TRY(mg_alloc(c, &L.w32, n));
+      UFC_TRY(mg_alloc(c, &L.x32, n));
+      UFC_TRY(mg_alloc(c, &L.b32, n));
+      UFC_TRY(mg_alloc(c, &L.val32, nv));
+      UFC_TRY(mg_alloc(c, &L.dinv32, n));
+      k_mg_round<<<grid_n(nv), kBlk, 0, c->stream>>>(nv, L.c->val64, L.val32);
+      k_mg_round<<<grid_n(n), kBlk, 0, c->stream>>>(n, L.c->dinv64, L.dinv32);
+    } else {
+      UFC_TRY(mg_alloc(c, &L.r, n));
+      UFC_TRY(mg_alloc(c, &L.d, n));
+      UFC_TRY(mg_alloc(c, &L.w, n));
+      if (l > 0) {
+        L.own_xb = true;
+        UFC_TRY(mg_alloc(c, &L.x, n));
+        UFC_TRY(mg_alloc(c, &L.b, n));
+      }
+    }
+    if (l + 1 < mg.lv.size() || n > 4096) UFC_TRY(estimate_lmax(c, L, 15));
+  }
+  MgLevel& Cst = mg.lv.back();
+  dfree(&Cst.inv);
+  dfree(&Cst.inv32);
+  if (Cst.c->n <= 4096) {
+    UFC_TRY(dense_inverse(c, Cst, mg.fp32));
+    mg.cheb_coarse = 0;
+  } else {
+    mg.cheb_coarse = 24;
+  }
+  mg.stale = false;
+  return UFC_STATUS_OK;
 }
 
 int mg_setup(Ctx* c, ufc_mg_arg* a) {
@@ -610,7 +795,7 @@ int mg_setup(Ctx* c, ufc_mg_arg* a) {
   Mg& mg = *c->mg;
   mg.degree = a->degree > 0 ? a->degree : 2;
   mg.ratio = a->ratio > 1.0 ? a->ratio : 15.0;
-  const int64_t coarse_max = a->coarse_max > 0 ? a->coarse_max : 1000;
+  const int64_t coarse_max = a->coarse_max > 0 ? a->coarse_max : 300;
   const int max_levels = a->max_levels > 0 ? a->max_levels : 32;
   auto bail = [&](int s) {
     mg_free(c);
@@ -684,85 +869,22 @@ int mg_setup(Ctx* c, ufc_mg_arg* a) {
   }
   if (mg.lv.size() < 2) return bail(fail(c, UFC_STATUS_INVALID, "ufc_mg_setup: the box cannot be coarsened"));
 
-  // Galerkin element matrices and coarse matrices, level by level
-  for (size_t l = 1; l < mg.lv.size(); ++l) {
-    MgLevel& F = mg.lv[l - 1];
-    MgLevel& L = mg.lv[l];
-    Ctx* lc = L.c;
-    if (dalloc(c, &L.ke, (int64_t)lc->E * 576) != UFC_STATUS_OK) return bail(UFC_STATUS_MEM_ERROR);
-    const int grid = lc->E;
-    if (l == 1) {
-      if (tangent)
-        k_mg_galerkin<false, true><<<grid, 64, 0, c->stream>>>(L.nx, L.ny, L.nz, c->coords, c->conn, c->props,
-                                                               c->nprops, c->Dt, nullptr, c->fixed, lc->conn,
-                                                               lc->fixed, L.ke, c->dev_err);
-      else
-        k_mg_galerkin<false, false><<<grid, 64, 0, c->stream>>>(L.nx, L.ny, L.nz, c->coords, c->conn, c->props,
-                                                                c->nprops, nullptr, nullptr, c->fixed, lc->conn,
-                                                                lc->fixed, L.ke, c->dev_err);
-    } else {
-      k_mg_galerkin<true, false><<<grid, 64, 0, c->stream>>>(L.nx, L.ny, L.nz, nullptr, F.c->conn, nullptr, 0,
-                                                             nullptr, F.ke, F.c->fixed, lc->conn, lc->fixed, L.ke,
-                                                             c->dev_err);
-    }
-    if (cudaGetLastError() != cudaSuccess) return bail(fail(c, UFC_STATUS_ERROR, "ufc_mg_setup: Galerkin launch"));
-    const int64_t nv = lc->sell_blocks * 9;
-    if (dalloc(c, &lc->val64, nv) != UFC_STATUS_OK || dinv_of(lc) != UFC_STATUS_OK) return bail(UFC_STATUS_MEM_ERROR);
-    cudaMemsetAsync(lc->val64, 0, sizeof(double) * nv, c->stream);
-    for (int col = 0; col < lc->ncol; ++col) {
-      const int32_t ne = lc->col_off[col + 1] - lc->col_off[col];
-      if (ne == 0) continue;
-      k_mg_scatter<<<(int)(((int64_t)ne * 64 + kBlk - 1) / kBlk), kBlk, 0, c->stream>>>(
-          lc->col_elems + lc->col_off[col], ne, lc->conn, L.ke, lc->slot, lc->fixed, lc->val64);
-    }
-    if (lc->nfix > 0)
-      k_mg_fix_diag<<<grid_for(lc->nfix, kBlk), kBlk, 0, c->stream>>>(lc->nfix, lc->fix_dofs, lc->dpos, lc->val64);
-    k_mg_dinv<<<grid_for(lc->n, kBlk), kBlk, 0, c->stream>>>(lc->N, lc->dpos, lc->val64, lc->dinv64);
-    if (cudaGetLastError() != cudaSuccess) return bail(fail(c, UFC_STATUS_ERROR, "ufc_mg_setup: coarse assembly"));
-    lc->has_val64 = true;
-  }
-  if (check_dev_err(c, "ufc_mg_setup") != UFC_STATUS_OK) return bail(UFC_STATUS_ERROR);
-
-  // level vectors, smoother bounds, coarsest solve
-  for (size_t l = 0; l < mg.lv.size(); ++l) {
-    MgLevel& L = mg.lv[l];
-    const int64_t n = L.c->n;
-    if (dalloc(c, &L.r, n) != UFC_STATUS_OK || dalloc(c, &L.d, n) != UFC_STATUS_OK ||
-        dalloc(c, &L.w, n) != UFC_STATUS_OK)
-      return bail(UFC_STATUS_MEM_ERROR);
-    if (l > 0) {
-      L.own_xb = true;
-      if (dalloc(c, &L.x, n) != UFC_STATUS_OK || dalloc(c, &L.b, n) != UFC_STATUS_OK)
-        return bail(UFC_STATUS_MEM_ERROR);
-    }
-    if (l + 1 < mg.lv.size() || n > 4096) {
-      const int s = estimate_lmax(c, L, 15);
-      if (s != UFC_STATUS_OK) return bail(s);
-    }
-  }
-  MgLevel& Cst = mg.lv.back();
-  if (Cst.c->n <= 4096) {
-    const int s = dense_inverse(c, Cst);
-    if (s != UFC_STATUS_OK) return bail(s);
-    mg.cheb_coarse = 0;
-  } else {
-    mg.cheb_coarse = 24;
+  mg.fp32 = a->precision == UFC_PRECISION_FP32_REFINE;
+  {
+    const int st = mg_numeric(c);
+    if (st != UFC_STATUS_OK) return bail(st);
   }
   a->levels = (int32_t)mg.lv.size();
-  a->coarse_dof = Cst.c->n;
+  a->coarse_dof = mg.lv.back().c->n;
   UFC_CUDA(c, cudaStreamSynchronize(c->stream));
   a->setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return UFC_STATUS_OK;
 }
 
 int mg_apply(Ctx* c, const double* r, double* z) {
-  if (!c->mg || c->mg->stale)
-    return fail(c, UFC_STATUS_INVALID, "ufc_mg_apply: multigrid not set up for the current matrix (ufc_mg_setup)");
-  Mg& mg = *c->mg;
-  MgLevel& L0 = mg.lv[0];
-  L0.b = const_cast<double*>(r);
-  L0.x = z;
-  vcycle(c, mg, 0, nullptr);
+  if (!c->mg) return fail(c, UFC_STATUS_INVALID, "ufc_mg_apply: multigrid not set up (ufc_mg_setup)");
+  if (c->mg->stale) UFC_TRY(mg_refresh(c));
+  run_cycle(c, *c->mg, r, z, nullptr);
   UFC_CUDA(c, cudaGetLastError());
   return UFC_STATUS_OK;
 }
@@ -774,15 +896,20 @@ int mg_level_ctx(Ctx* c, int32_t level, Ctx** out) {
   return UFC_STATUS_OK;
 }
 
+int mg_refresh(Ctx* c) {
+  if (!c->has_val64) return fail(c, UFC_STATUS_INVALID, "multigrid: the FP64 values are not assembled");
+  if (c->mat_model == UFC_MAT_J2_ISO && !c->has_trial)
+    return fail(c, UFC_STATUS_INVALID, "multigrid: J2 tangent needs ufc_elem_compute_fint(update_state=1) first");
+  release_graphs(c);
+  return mg_numeric(c);
+}
+
 int pcg_mg(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
-  if (!c->mg || c->mg->stale)
-    return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: multigrid not set up for the current matrix (ufc_mg_setup)");
+  if (!c->mg) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: multigrid not set up (ufc_mg_setup)");
+  if (c->mg->stale) UFC_TRY(mg_refresh(c));
   Mg& mg = *c->mg;
   if (!c->r64 || !c->p64 || !c->q64) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: vectors");
   if (!c->z64) UFC_TRY(dalloc(c, &c->z64, c->n));
-  MgLevel& L0 = mg.lv[0];
-  L0.b = c->r64;
-  L0.x = c->z64;
   const int64_t n = c->n;
   const int vg = grid_n(n);
   cudaEvent_t t0, t1;
@@ -824,7 +951,7 @@ int pcg_mg(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
     UFC_CUDA(c, cudaMemcpyAsync(&c->scal->tol2, &tol2, sizeof(double), cudaMemcpyHostToDevice, c->stream));
     UFC_CUDA(c, cudaMemsetAsync(&c->scal->stop, 0, sizeof(int32_t), c->stream));
     UFC_CUDA(c, cudaMemcpyAsync(c->r64, c->y64, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
-    vcycle(c, mg, 0, c->scal);
+    run_cycle(c, mg, c->r64, c->z64, c->scal);
     k_mgcg_rz<<<vg, kBlk, 0, c->stream>>>(n, c->r64, c->z64, c->scal, c->partials, 1);
     c->launches += 1;
     UFC_CUDA(c, cudaMemcpyAsync(c->p64, c->z64, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
@@ -835,7 +962,7 @@ int pcg_mg(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
       for (int b = 0; b < batch; ++b) {
         cg_spmv64(c, c->p64, c->q64);
         k_mgcg_update<<<vg, kBlk, 0, c->stream>>>(n, c->p64, c->q64, c->r64, c->x64, c->scal, c->partials);
-        vcycle(c, mg, 0, c->scal);
+        run_cycle(c, mg, c->r64, c->z64, c->scal);
         k_mgcg_rz<<<vg, kBlk, 0, c->stream>>>(n, c->r64, c->z64, c->scal, c->partials, 0);
         k_mgcg_pupdate<<<vg, kBlk, 0, c->stream>>>(n, c->z64, c->p64, c->scal);
         c->launches += 4;

@@ -849,6 +849,10 @@ void spmv64_on(const Ctx* lvl, cudaStream_t st, const double* x, double* y) {
   launch_spmv<double, double, double, kPlain>(lvl, st, lvl->val64, x, y);
 }
 
+void spmv32_on(const Ctx* lvl, cudaStream_t st, const float* val, const float* x, float* y) {
+  launch_spmv_diff<float, float, float, kPlain, false>(lvl, st, val, x, y);
+}
+
 void cg_spmv64(Ctx* c, const double* p, double* q) {
   launch_spmv<double, double, double, kCg>(c, c->stream, c->val64, p, q);
 }

@@ -185,6 +185,8 @@ int mg_level_ctx(Ctx* c, int32_t level, Ctx** out);
 int pcg_mg(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st);
 // FP64 SELL SpMV (full storage) of any context's values, on the given stream (solver.cu)
 void spmv64_on(const Ctx* lvl, cudaStream_t st, const double* x, double* y);
+// FP32 SELL SpMV of the given values (standard form) on any context's pattern
+void spmv32_on(const Ctx* lvl, cudaStream_t st, const float* val, const float* x, float* y);
 void cg_spmv64(Ctx* c, const double* p, double* q);  // q = K p, p.q and alpha = r.z / p.q into the scalars
 int true_residual_fp64(Ctx* c, bool want_bb);  // y64 = b64 - K x64, scal->true_rr (and bb)
 

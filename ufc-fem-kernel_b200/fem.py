@@ -343,13 +343,14 @@ class FemModel:
         return X, [SolverState.from_c(s, st) for s in cs]
 
     # ---------------------------------------------------------------- multigrid
-    def mg_setup(self, nx, ny, nz, max_levels=0, degree=0, ratio=0.0, coarse_max=0):
+    def mg_setup(self, nx, ny, nz, max_levels=0, degree=0, ratio=0.0, coarse_max=0, precision=A.PRECISION_FP64):
         """Geometric multigrid hierarchy of the nx x ny x nz box (ufc_mg_setup);
-        solve with SolverAlgo(precond_type=SOLV_PREC_MG).  Returns
-        (levels, coarsest DOF, set-up ms)."""
+        solve with SolverAlgo(precond_type=SOLV_PREC_MG).  precision
+        PRECISION_FP32_REFINE runs the cycle in FP32.  Returns (levels,
+        coarsest DOF, set-up ms)."""
         a = A.MgArg()
         a.nx, a.ny, a.nz, a.max_levels, a.degree = int(nx), int(ny), int(nz), int(max_levels), int(degree)
-        a.ratio, a.coarse_max = float(ratio), int(coarse_max)
+        a.ratio, a.coarse_max, a.precision = float(ratio), int(coarse_max), int(precision)
         self._check(self.lib.ufc_mg_setup(self.h, C.byref(a)), "ufc_mg_setup")
         return a.levels, a.coarse_dof, a.setup_ms
 
