@@ -17,7 +17,7 @@ MODULE ufc_gpu_brg
 
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_MEM_HOST = 0, UFC_MEM_DEVICE = 1
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_MAT_ELASTIC_ISO = 101, UFC_MAT_J2_ISO = 201
-  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_SOLV_METHOD_CG = 3, UFC_SOLV_PREC_JACOBI = 1
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_SOLV_METHOD_CG = 3, UFC_SOLV_PREC_JACOBI = 1, UFC_SOLV_PREC_MG = 5
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_PRECISION_FP64 = 0, UFC_PRECISION_FP32_REFINE = 1
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_BUILD_FP64 = 1, UFC_BUILD_FP32 = 2
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_BUILD_FP32_ROUNDED = 4, UFC_BUILD_FP32_DIFF = 8
@@ -107,6 +107,15 @@ MODULE ufc_gpu_brg
     INTEGER(C_INT32_T)    :: completed, status
   END TYPE
 
+  TYPE, BIND(C), PUBLIC :: ufc_mg_arg               ! multigrid in the place of NM_AMG_Setup
+    INTEGER(C_INT32_T)    :: nx, ny, nz, max_levels = 0, degree = 0
+    REAL(C_DOUBLE)        :: ratio = 0.0D0
+    INTEGER(C_INT64_T)    :: coarse_max = 0
+    INTEGER(C_INT32_T)    :: levels, precision = 0
+    INTEGER(C_INT64_T)    :: coarse_dof
+    REAL(C_DOUBLE)        :: setup_ms
+  END TYPE
+
   TYPE, BIND(C), PUBLIC :: ufc_face_load_arg        ! PH_Elem_C3D8_FormFacePressure over a face set
     INTEGER(C_INT32_T)    :: n_faces
     TYPE(C_PTR)           :: elem, face, traction, pressure
@@ -118,7 +127,7 @@ MODULE ufc_gpu_brg
   PUBLIC :: ufc_pattern_build, ufc_csr_export, ufc_elem_compute_ke, ufc_elem_compute_fint
   PUBLIC :: ufc_mat_update_batch, ufc_pcg_solve, ufc_pcg_solve_block, ufc_nr_increment
   PUBLIC :: ufc_state_commit, ufc_state_rollback, ufc_get_displacement, ufc_adjoint_sensitivity
-  PUBLIC :: ufc_nr_step, ufc_load_faces, ufc_stress_nodal, ufc_reactions
+  PUBLIC :: ufc_nr_step, ufc_load_faces, ufc_stress_nodal, ufc_reactions, ufc_mg_setup, ufc_mg_apply
 
   INTERFACE
     INTEGER(C_INT) FUNCTION ufc_ctx_create(device, ctx) BIND(C, NAME='ufc_ctx_create')
@@ -205,6 +214,18 @@ MODULE ufc_gpu_brg
       IMPORT :: C_INT, C_PTR, ufc_step_arg
       TYPE(C_PTR), VALUE                 :: ctx
       TYPE(ufc_step_arg), INTENT(INOUT)  :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_mg_setup(ctx, arg) BIND(C, NAME='ufc_mg_setup')
+      IMPORT :: C_INT, C_PTR, ufc_mg_arg
+      TYPE(C_PTR), VALUE               :: ctx
+      TYPE(ufc_mg_arg), INTENT(INOUT)  :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_mg_apply(ctx, r, z, mem) BIND(C, NAME='ufc_mg_apply')
+      IMPORT :: C_INT, C_PTR, C_DOUBLE, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx
+      REAL(C_DOUBLE), INTENT(IN)    :: r(*)
+      REAL(C_DOUBLE), INTENT(OUT)   :: z(*)
+      INTEGER(C_INT32_T), VALUE     :: mem
     END FUNCTION
     INTEGER(C_INT) FUNCTION ufc_load_faces(ctx, arg) BIND(C, NAME='ufc_load_faces')
       IMPORT :: C_INT, C_PTR, ufc_face_load_arg
