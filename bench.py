@@ -176,9 +176,11 @@ def make_problem(args):
     return ufc, ufc.mesh.lognormal_cantilever(nx, ny, nz, seed=4)
 
 
-def cpu_sample(p, iters, reps=1):
+def cpu_sample(p, iters, reps=1, check=None):
     """Oracle (CPU FP64, all host threads) per-iteration time of Jacobi-PCG on the
-    problem's canonical CSR: setup time, seconds per iteration."""
+    problem's canonical CSR: setup time, seconds per iteration, threads, and for
+    each GPU solution in `check` (name -> host array) its relative residual
+    ||b - K u|| / ||b|| with the oracle's own assembly and right-hand side."""
     from oracle import oracle as O
 
     t0 = time.perf_counter()
@@ -191,7 +193,11 @@ def cpu_sample(p, iters, reps=1):
         t = time.perf_counter()
         O.pcg(K, b, max_iter=-iters)
         per.append((time.perf_counter() - t) / iters)
-    return setup, per, O.num_threads()
+    import numpy as np
+
+    bn = float(np.linalg.norm(b))
+    res = {k: float(np.linalg.norm(b - K.matvec(u)) / bn) for k, u in (check or {}).items()}
+    return setup, per, O.num_threads(), res
 
 
 def other_configs(ufc, local, stream):
@@ -498,8 +504,12 @@ def run_ours(args):
                  "traffic": profile_traffic("spmv_sell_fp32_192x96x96.txt")}
 
     cpu = None
+    oracle_res = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        setup, per, threads = cpu_sample(p, args.cpu_iters)
+        checks = {"fp32_refine": u_mixed.cpu().numpy(), "fp64": u_fp64.cpu().numpy()}
+        if mg_line and "value" in mg_line:
+            checks["multigrid"] = u_mg.cpu().numpy()
+        setup, per, threads, oracle_res = cpu_sample(p, args.cpu_iters, check=checks)
         iters64 = fst.niter
         cpu = {"value": per[0] * iters64, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{args.cpu_iters} FP64 Jacobi-PCG iterations of the oracle (OpenMP, canonical CSR) on "
@@ -546,6 +556,10 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if oracle_res:
+        # the GPU solutions checked with the oracle's CPU assembly of the same problem
+        line["accuracy_vs_oracle"] = {"residual_rel": oracle_res,
+                                      "note": "||b - K u|| / ||b|| with the oracle's canonical CSR and lifted b"}
     if other:
         line["other_storage"] = other
     if mg_line:

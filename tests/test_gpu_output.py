@@ -129,3 +129,24 @@ def test_reactions_balance_and_match_oracle(pkg, orc):
     np.testing.assert_allclose(rf, ref, rtol=0, atol=1e-10 * np.abs(ref).max())
     m.set_displacement(u)
     np.testing.assert_array_equal(m.reactions(f_ext=p.f), rf)
+
+
+def test_edge_cases(pkg):
+    p = pkg.mesh.j2_bar(3, 2, 2)
+    m = pkg.FemModel.from_problem(p)
+    # no faces: a zero load vector
+    f = m.load_faces(np.zeros(0, dtype=np.int32), np.zeros(0, dtype=np.int32), traction=np.zeros((0, 3)))
+    assert f.shape == (p.n_dof,) and not f.any()
+    # element id out of range
+    with pytest.raises(pkg.UfcError) as ei:
+        m.load_faces([p.n_elems], [1], pressure=[1.0])
+    assert ei.value.status_code == 1
+    # J2 before any increment: zero committed stress at the nodes, zero reactions
+    sig, vm = m.stress_nodal()
+    assert not sig.any() and not vm.any()
+    assert not m.reactions().any()
+    # invalid increment controls are rejected before any work
+    for bad in (dict(cutback_factor=1.5), dict(dt_initial=0.0), dict(max_iterations=0), dict(dt_min=2.0)):
+        with pytest.raises(pkg.UfcError) as ei:
+            m.nr_step(pkg.mesh.j2_bar_target(p, 1, n_steps=1), **bad)
+        assert ei.value.status_code == 1, bad
