@@ -287,6 +287,21 @@ __global__ void __launch_bounds__(kSpmvBlock)
     };
     const int mlen = ulen < llen ? ulen : llen;
     int j = 0;
+    // four steps per trip for FP64 values, two for FP32 (each the faster of the
+    // two on B200, measured in the CG)
+    if constexpr (sizeof(TV) == 8) {
+#pragma unroll 1
+      for (; j + 3 < mlen; j += 4) {
+        upper(j);
+        lower(j);
+        upper(j + 1);
+        lower(j + 1);
+        upper(j + 2);
+        lower(j + 2);
+        upper(j + 3);
+        lower(j + 3);
+      }
+    }
 #pragma unroll 1
     for (; j + 1 < mlen; j += 2) {
       upper(j);
