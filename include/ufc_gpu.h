@@ -299,7 +299,7 @@ typedef struct {
  * level (a coarse DOF is fixed when its coincident fine DOF is).  Smoother:
  * Chebyshev polynomial of D^-1 A of the given degree before and after the
  * coarse correction, on [lambda_max/ratio, 1.1 lambda_max] with lambda_max
- * from a power iteration; coarsest level: dense inverse (<= 4096 DOF) or a
+ * from a power iteration; coarsest level: dense inverse (<= 1200 DOF) or a
  * degree-24 Chebyshev solve.  Uses the assembled FP64 values (and, for J2, the
  * tangent of the trial state): call it after ufc_elem_compute_ke; after a
  * reassembly the numerical part (coarse operators, smoother bounds, coarsest

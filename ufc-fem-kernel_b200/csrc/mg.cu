@@ -19,7 +19,7 @@
 // Cycle.  V-cycle with a Chebyshev polynomial smoother of D^-1 A (same degree
 // before and after the coarse correction, so the preconditioner is symmetric),
 // on [lambda_max/ratio, 1.1 lambda_max] with lambda_max from a power iteration
-// at set-up; the coarsest level is solved with its dense inverse (<= 4096 DOF)
+// at set-up; the coarsest level is solved with its dense inverse (<= kDenseMax DOF)
 // or a high-degree Chebyshev polynomial.  Restriction and prolongation are
 // structured gathers, one thread per coarse or fine node, so they need no
 // atomics and are deterministic; the coarse matrices are assembled colour by
@@ -74,6 +74,9 @@ struct Mg {
 namespace {
 
 constexpr int kBlk = 256;
+// largest coarsest level inverted densely (on the host, O(n^3), at every set-up
+// and refresh); larger ones get a degree-24 Chebyshev solve
+constexpr int64_t kDenseMax = 1200;
 
 int grid_n(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + kBlk - 1) / kBlk, 148 * 16)); }
 
@@ -752,12 +755,12 @@ int mg_numeric(Ctx* c) {
         UFC_TRY(mg_alloc(c, &L.b, n));
       }
     }
-    if (l + 1 < mg.lv.size() || n > 4096) UFC_TRY(estimate_lmax(c, L, 15));
+    if (l + 1 < mg.lv.size() || n > kDenseMax) UFC_TRY(estimate_lmax(c, L, 15));
   }
   MgLevel& Cst = mg.lv.back();
   dfree(&Cst.inv);
   dfree(&Cst.inv32);
-  if (Cst.c->n <= 4096) {
+  if (Cst.c->n <= kDenseMax) {
     UFC_TRY(dense_inverse(c, Cst, mg.fp32));
     mg.cheb_coarse = 0;
   } else {
