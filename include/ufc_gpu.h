@@ -199,7 +199,7 @@ typedef struct {
 /* NM_Solver_Algo (ufc_core/L2_NM/Solver/NM_Solv_Def.f90:86-100). */
 typedef struct {
   int32_t method;         /* [IN] UFC_SOLV_METHOD_CG */
-  int32_t precond_type;   /* [IN] UFC_SOLV_PREC_JACOBI or UFC_SOLV_PREC_NONE */
+  int32_t precond_type;   /* [IN] UFC_SOLV_PREC_JACOBI, UFC_SOLV_PREC_MG (after ufc_mg_setup) or UFC_SOLV_PREC_NONE */
   int32_t max_iter;       /* [IN] */
   int32_t precision_mode; /* [IN] UFC_PRECISION_FP64 or UFC_PRECISION_FP32_REFINE */
   double tolerance;       /* [IN] stop when ||b - K x||_2 <= max(tolerance*||b||_2, abs_tolerance) */
