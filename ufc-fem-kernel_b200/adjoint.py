@@ -8,7 +8,8 @@ the GPU with P the projection onto the free DOFs (Dirichlet values are zero).
 Any scalar objective built from U and F by torch ops differentiates through it:
 compliance J = sum(F * U), a tip displacement U[..., dof], ...
 
-backward(gU) solves K Lam = P gU with the same Jacobi-PCG (K is symmetric),
+backward(gU) solves K Lam = P gU with the same PCG (Jacobi or multigrid
+preconditioner, as algo says; K is symmetric),
 reusing the stiffness assembled in forward and the saved U (nothing is
 reassembled while E is unchanged), then evaluates
 dJ/dE_e = -sum_k Lam_k,e^T (dK_e/dE_e) U_k,e for all elements in one kernel
