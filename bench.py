@@ -200,8 +200,44 @@ def cpu_sample(p, iters, reps=1, check=None):
     return setup, per, O.num_threads(), res
 
 
+def linear_static(ufc, local, p):
+    """Time-to-rtol 1e-10 of one linear-elastic problem from x0 = 0: FP64
+    Jacobi-PCG, the FP32+FP64-refined one (full storage) and FP64 PCG with the
+    multigrid preconditioner, each timed by the library's CUDA events after one
+    warm-up solve, with the assembly time."""
+    import torch
+
+    dev = torch.device("cuda", local)
+    m = ufc.FemModel.from_problem(p, device=local)
+    ka = m.assemble(ufc.BUILD_FP64 | ufc.BUILD_FP32_ROUNDED)
+    b = torch.from_numpy(ufc.lifted_rhs(m, p.f)).to(dev)
+    x = torch.zeros_like(b)
+    res = {"n_dof": p.n_dof, "elements": p.n_elems, "assembly_ms": ka}
+    for key, pm in (("fp64", ufc.PRECISION_FP64), ("fp32_refine", ufc.PRECISION_FP32_REFINE)):
+        a = ufc.SolverAlgo(tolerance=1e-10, precision_mode=pm)
+        x.zero_()
+        m.solve(b, a, x=x, raise_on_not_converged=False)
+        x.zero_()
+        _, st = m.solve(b, a, x=x, raise_on_not_converged=False)
+        res[key] = {"s": st.solve_time / 1e3, "iters": st.niter, "rnorm": st.rnorm, "converged": st.converged}
+        if pm != ufc.PRECISION_FP64:
+            res[key]["fp64_continuation_iters"] = st.fp64_iters
+    # FP64 PCG with the geometric multigrid V-cycle in FP32 (set-up outside the timed solve)
+    levels, coarse, setup_ms = m.mg_setup(*p.shape, precision=ufc.PRECISION_FP32_REFINE)
+    a = ufc.SolverAlgo(tolerance=1e-10, precond_type=ufc.SOLV_PREC_MG)
+    x.zero_()
+    m.solve(b, a, x=x, raise_on_not_converged=False)
+    x.zero_()
+    _, st = m.solve(b, a, x=x, raise_on_not_converged=False)
+    res["multigrid"] = {"s": st.solve_time / 1e3, "iters": st.niter, "rnorm": st.rnorm, "converged": st.converged,
+                        "levels": levels, "coarsest_dof": coarse, "setup_s": setup_ms / 1e3}
+    m.close()
+    return res
+
+
 def other_configs(ufc, local, stream):
-    """The two other device workloads of the path, timed once each with CUDA events:
+    """The other device workloads of the path, timed with CUDA events: the
+    40x8x8 cantilever and the 128x64x64 lognormal cantilever (linear static),
     the 64x32x32 J2 bar pulled to 1 % strain in 20 Newton-Raphson increments, and
     16 tip-load cases of the 128x64x64 density problem solved as one block PCG
     plus the adjoint sensitivity dJ/dE of every element."""
@@ -209,6 +245,11 @@ def other_configs(ufc, local, stream):
 
     dev = torch.device("cuda", local)
     out = {}
+    for key, make in (("cantilever_40x8x8", ufc.mesh.config1), ("lognormal_128x64x64", ufc.mesh.config2)):
+        try:
+            out[key] = linear_static(ufc, local, make())
+        except Exception as e:  # a failure here must not lose the headline line
+            out[key] = {"error": f"{type(e).__name__}: {e}"}
     try:
         p = ufc.mesh.config3()
         m = ufc.FemModel.from_problem(p, device=local)

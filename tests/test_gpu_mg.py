@@ -101,21 +101,34 @@ def test_vcycle_symmetric_positive(pkg):
     np.testing.assert_array_equal(m.mg_apply(a), Ma)  # deterministic
 
 
+@pytest.mark.parametrize("storage", ["full", "symmetric"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("name,make,dims", [
     ("cantilever_40x8x8", lambda mesh: mesh.config1(), (40, 8, 8)),
     ("lognormal_32x16x16", lambda mesh: mesh.lognormal_cantilever(32, 16, 16, seed=2), (32, 16, 16)),
 ])
-def test_mg_pcg_matches_jacobi(pkg, orc, name, make, dims, precision):
+def test_mg_pcg_matches_jacobi(pkg, orc, name, make, dims, precision, storage):
     """FP64 PCG around the V-cycle, the cycle in FP64 or FP32: the answer has
-    the FP64 residual either way."""
+    the FP64 residual either way.  With symmetric storage the finest level's
+    products (outer PCG, smoother, residual) take the half storage."""
     p = make(pkg.mesh)
     m = pkg.FemModel.from_problem(p)
-    m.assemble(pkg.BUILD_FP64)
+    sym = pkg.BUILD_FP32_ROUNDED | pkg.BUILD_SYMMETRIC if storage == "symmetric" else 0
+    m.assemble(pkg.BUILD_FP64 | sym)
     prec = pkg.PRECISION_FP64 if precision == "fp64" else pkg.PRECISION_FP32_REFINE
     levels, cdof, _ = m.mg_setup(*dims, precision=prec)
     assert levels >= 3
     b = pkg.lifted_rhs(m, p.f)
+    if sym:
+        # the cycle on the half storage is the cycle on the full storage, up to
+        # the order of the row sums
+        f = pkg.FemModel.from_problem(p)
+        f.assemble(pkg.BUILD_FP64)
+        f.mg_setup(*dims, precision=prec)
+        r = np.random.default_rng(3).standard_normal(p.n_dof)
+        zs, zf = m.mg_apply(r), f.mg_apply(r)
+        np.testing.assert_allclose(zs, zf, rtol=0, atol=(1e-11 if precision == "fp64" else 1e-4) * np.abs(zf).max())
+        f.close()
     xj, sj = m.solve(b, pkg.SolverAlgo(tolerance=1e-10))
     xm, sm = m.solve(b, pkg.SolverAlgo(tolerance=1e-10, precond_type=pkg.SOLV_PREC_MG))
     assert sm.converged and sm.rnorm <= 1e-10

@@ -552,7 +552,7 @@ Vecs<TV, TX> vecs(Ctx* c, bool precond) {
 }
 
 template <typename TV, typename TX, typename TA, int MODE>
-void launch_spmv_sym(Ctx* c, int grid, cudaStream_t st, const TV* val, const TX* x, TX* y) {
+void launch_spmv_sym(const Ctx* c, int grid, cudaStream_t st, const TV* val, const TX* x, TX* y) {
   k_spmv_sym<TV, TX, TA, MODE><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->uptr, c->ucol, c->lptr,
                                                             c->lpos, c->lcol, val, x, y, c->scal, c->partials);
 }
@@ -887,20 +887,35 @@ int64_t spmv_bytes(const Ctx* c, int precision) {
   return c->nnzb * (9 * sv + 4) + 4 * ((int64_t)c->N + 1) + 2 * c->n * sx;
 }
 
+int sym_grid(const Ctx* c) { return (int)((c->nslices * kSlice + kSpmvBlock - 1) / kSpmvBlock); }
+
+// The products of the multigrid cycle and of its outer PCG take the symmetric
+// storage of a level when it holds current values (the finest level of a model
+// assembled with UFC_BUILD_SYMMETRIC: FP64 values and the same values rounded
+// to FP32, as the cycle's own FP32 copy), else the full SELL storage.
 void spmv64_on(const Ctx* lvl, cudaStream_t st, const double* x, double* y) {
-  launch_spmv<double, double, double, kPlain>(lvl, st, lvl->val64, x, y);
+  if (lvl->has_sval64)
+    launch_spmv_sym<double, double, double, kPlain>(lvl, sym_grid(lvl), st, lvl->sval64, x, y);
+  else
+    launch_spmv<double, double, double, kPlain>(lvl, st, lvl->val64, x, y);
 }
 
 void spmv32_on(const Ctx* lvl, cudaStream_t st, const float* val, const float* x, float* y) {
-  launch_spmv_diff<float, float, float, kPlain, false>(lvl, st, val, x, y);
+  if (lvl->has_sval32)
+    launch_spmv_sym<float, float, float, kPlain>(lvl, sym_grid(lvl), st, lvl->sval32, x, y);
+  else
+    launch_spmv_diff<float, float, float, kPlain, false>(lvl, st, val, x, y);
 }
 
 void cg_spmv64(Ctx* c, const double* p, double* q) {
-  launch_spmv<double, double, double, kCg>(c, c->stream, c->val64, p, q);
+  if (c->has_sval64)
+    launch_spmv_sym<double, double, double, kCg>(c, sym_grid(c), c->stream, c->sval64, p, q);
+  else
+    launch_spmv<double, double, double, kCg>(c, c->stream, c->val64, p, q);
 }
 
 int true_residual_fp64(Ctx* c, bool want_bb) {
-  launch_spmv<double, double, double, kPlain>(c, c->stream, c->val64, c->x64, c->y64);
+  spmv64_on(c, c->stream, c->x64, c->y64);
   UFC_CUDA(c, cudaGetLastError());
   k_resid<<<vec_grid(c->n), kVecBlock, 0, c->stream>>>(c->n, c->b64, c->y64, c->y64, c->scal, c->partials,
                                                        want_bb ? 1 : 0);
