@@ -252,50 +252,48 @@ def other_configs(ufc, local, stream):
             out[key] = {"error": f"{type(e).__name__}: {e}"}
     try:
         p = ufc.mesh.config3()
-        m = ufc.FemModel.from_problem(p, device=local)
-        lin = ufc.SolverAlgo(tolerance=1e-10)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        torch.cuda.synchronize(dev)
-        ev[0].record(stream)
-        nr_iters = lin_iters = 0
-        ok = True
-        for s in range(1, 21):
-            res = m.nr_increment(ufc.mesh.j2_bar_target(p, s), tolerance_force=1e-8, lin=lin)
-            ok = ok and res.converged
-            nr_iters += res.iterations
-            lin_iters += res.lin_iters_total
-            m.commit()
-        ev[1].record(stream)
-        torch.cuda.synchronize(dev)
+
+        def j2_run(multigrid, n_steps):
+            """The first n_steps of the 20 increments on a fresh model, timed with
+            CUDA events: (seconds, converged, Newton iterations, CG iterations)."""
+            m = ufc.FemModel.from_problem(p, device=local)
+            lin = ufc.SolverAlgo(tolerance=1e-10)
+            if multigrid:  # hierarchy built once, its numbers rebuilt after every tangent assembly
+                m.internal_force(m.displacement(), update_state=True)
+                m.assemble(ufc.BUILD_FP64)
+                m.mg_setup(*p.shape)
+                lin = ufc.SolverAlgo(tolerance=1e-10, precond_type=ufc.SOLV_PREC_MG)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            torch.cuda.synchronize(dev)
+            ev[0].record(stream)
+            nr_iters = lin_iters = 0
+            ok = True
+            for s in range(1, n_steps + 1):
+                res = m.nr_increment(ufc.mesh.j2_bar_target(p, s), tolerance_force=1e-8, lin=lin)
+                ok = ok and res.converged
+                nr_iters += res.iterations
+                lin_iters += res.lin_iters_total
+                m.commit()
+            ev[1].record(stream)
+            torch.cuda.synchronize(dev)
+            m.close()
+            return ev[0].elapsed_time(ev[1]) / 1e3, ok, nr_iters, lin_iters
+
+        # warm-up: the first elastic and plastic increments of each variant on a
+        # throwaway model (first kernel launches, graph paths), then the timed run
+        for mg in (False, True):
+            j2_run(mg, 5)
+        t, ok, nr_iters, lin_iters = j2_run(False, 20)
         out["j2_bar_64x32x32"] = {
             "workload": "J2 bar 64x32x32 (E 200e3, nu 0.3, sy 250, H 1000), 20 displacement increments to 1 % "
                         "strain, NR to ||r|| <= 1e-8 max(||F_ext||,||F_int||), FP64 PCG rtol 1e-10 per iteration",
-            "s": ev[0].elapsed_time(ev[1]) / 1e3, "converged": ok, "nr_iterations": nr_iters,
+            "s": t, "converged": ok, "nr_iterations": nr_iters,
             "pcg_iterations": lin_iters, "n_dof": p.n_dof, "preconditioner": "Jacobi"}
-        m.close()
-        # the same increments with the multigrid preconditioner (hierarchy rebuilt per tangent)
-        m = ufc.FemModel.from_problem(p, device=local)
-        m.internal_force(m.displacement(), update_state=True)
-        m.assemble(ufc.BUILD_FP64)
-        m.mg_setup(*p.shape)
-        lin_mg = ufc.SolverAlgo(tolerance=1e-10, precond_type=ufc.SOLV_PREC_MG)
-        torch.cuda.synchronize(dev)
-        ev[0].record(stream)
-        nr_iters = lin_iters = 0
-        ok = True
-        for s in range(1, 21):
-            res = m.nr_increment(ufc.mesh.j2_bar_target(p, s), tolerance_force=1e-8, lin=lin_mg)
-            ok = ok and res.converged
-            nr_iters += res.iterations
-            lin_iters += res.lin_iters_total
-            m.commit()
-        ev[1].record(stream)
-        torch.cuda.synchronize(dev)
+        t, ok, nr_iters, lin_iters = j2_run(True, 20)
         out["j2_bar_64x32x32_multigrid"] = {
-            "s": ev[0].elapsed_time(ev[1]) / 1e3, "converged": ok, "nr_iterations": nr_iters,
+            "s": t, "converged": ok, "nr_iterations": nr_iters,
             "pcg_iterations": lin_iters, "preconditioner": "geometric multigrid (FP64 V-cycle), numerics rebuilt "
                                                           "after every tangent assembly"}
-        m.close()
     except Exception as e:  # a failure here must not lose the headline line
         out["j2_bar_64x32x32"] = {"error": f"{type(e).__name__}: {e}"}
     try:
