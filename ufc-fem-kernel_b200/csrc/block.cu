@@ -218,6 +218,167 @@ __global__ void __launch_bounds__(kBlk, 4)
   }
 }
 
+// Asynchronous copies global -> shared (cp.async): the data lands in shared
+// memory without occupying registers while in flight; a thread waits for its
+// own groups (wait_group) and a warp barrier publishes them to the warp.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async16ca(void* sdst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// One step of a warp task in shared memory: the 9 values of the RPW rows'
+// stored blocks (component-major, as in the SELL layout), shared by the warp,
+// and each lane's own x entries (3 components x its 2 right-hand sides) of the
+// step's column.
+template <int RPW>
+struct __align__(16) BStage {
+  double v[9][RPW];
+  double xs[32][3][2];
+};
+
+constexpr int kPipeD = 4;     // steps in flight per warp
+constexpr int kPipeLMax = 32;  // columns staged per chunk of a task
+
+template <int RPW>
+constexpr size_t bpipe_smem() {
+  return (size_t)kWarps * (kPipeD * sizeof(BStage<RPW>) + (size_t)kPipeLMax * RPW * sizeof(int32_t));
+}
+
+// Copies of local step jj of a chunk into a ring stage (none past the chunk);
+// every call commits one group, so the group count stays the step count.
+// The values of rows t0..t0+RPW-1 of step j sit at vp + 288 j + 32 c (16-byte
+// aligned: slice bases are multiples of 32 entries and t0 of RPW >= 2); the
+// lane's x entries at x + (3 col + comp) nr + k0 (k0 and nr even).
+template <int RPW>
+__device__ __forceinline__ void bstage_issue(BStage<RPW>& st, int lane, int rl, int k0, int jj, int cl,
+                                             const double* vp, const int32_t (*cols)[RPW],
+                                             const double* __restrict__ x, int nr) {
+  if (jj < cl) {
+    constexpr int kH = RPW / 2;
+    const double* vs = vp + 288 * (int64_t)jj;
+    for (int q = lane; q < 9 * kH; q += 32) {
+      const int cc = q / kH, h = q - cc * kH;
+      cp_async16(&st.v[cc][2 * h], vs + 32 * cc + 2 * h);
+    }
+    const int64_t cj = cols[jj][rl];
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) cp_async16ca(&st.xs[lane][comp][0], x + (3 * cj + comp) * nr + k0);
+  }
+  cp_commit();
+}
+
+// The block SpMV of k_bspmv for G = 2 and 4..32 right-hand sides (RPW = 32 /
+// tpr rows per warp task), software-pipelined through shared memory: a task's
+// columns are staged first (chunks of 32 steps), then each warp keeps the
+// values and its x lines of the next kPipeD steps in flight as asynchronous
+// copies into a ring, so that neither the matrix stream nor the dependent x
+// gathers hold registers while they wait.  The register-resident version keeps
+// a step's 9 values in 18 registers per lane and its x one step ahead, which
+// caps its loads in flight (latency-bound at about a fifth of the DRAM
+// bandwidth).  Same products in the same order as k_bspmv, same reduction.
+template <int RPW, int MODE>
+__global__ void __launch_bounds__(kBlk, 3)
+    k_bspmv_pipe(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
+                 const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y, int nr,
+                 BScalars* __restrict__ s, double* __restrict__ partials) {
+  constexpr int TPR = 32 / RPW;
+  constexpr int D = kPipeD;
+  extern __shared__ __align__(16) unsigned char bsm[];
+  if (MODE == 1 && s->stop) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rl = lane / TPR;
+  const int k0 = (lane % TPR) * 2;
+  BStage<RPW>* ring = reinterpret_cast<BStage<RPW>*>(bsm) + w * D;
+  int32_t(*cols)[RPW] = reinterpret_cast<int32_t(*)[RPW]>(bsm + kWarps * D * sizeof(BStage<RPW>) +
+                                                          (size_t)w * kPipeLMax * RPW * sizeof(int32_t));
+  double dot[1][2] = {{0.0, 0.0}};
+  const int64_t tasks = nslices * TPR;
+  const int64_t wstride = ((int64_t)gridDim.x * kBlk) >> 5;
+  for (int64_t task = ((int64_t)blockIdx.x * kBlk + threadIdx.x) >> 5; task < tasks; task += wstride) {
+    const int64_t sl = task / TPR;
+    const int t0 = (int)(task % TPR) * RPW;
+    const int64_t row = sl * kSlice + t0 + rl;
+    const int64_t base = sptr[sl];
+    const int len = (int)((sptr[sl + 1] - base) >> 5);
+    double acc[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int c0 = 0; c0 < len; c0 += kPipeLMax) {
+      const int cl = len - c0 < kPipeLMax ? len - c0 : kPipeLMax;
+      // the chunk's columns: lane l stages the RPW columns of step c0 + l
+      if (lane < cl) {
+        const int32_t* cs = col + base + t0 + 32 * (int64_t)(c0 + lane);
+        if constexpr (RPW >= 4) {
+#pragma unroll
+          for (int q = 0; q < RPW / 4; ++q)
+            *reinterpret_cast<int4*>(&cols[lane][4 * q]) = __ldcs(reinterpret_cast<const int4*>(cs) + q);
+        } else {
+          *reinterpret_cast<int2*>(&cols[lane][0]) = __ldcs(reinterpret_cast<const int2*>(cs));
+        }
+      }
+      __syncwarp();
+      const double* vp = val + 9 * (base + 32 * (int64_t)c0) + t0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) bstage_issue<RPW>(ring[d], lane, rl, k0, d, cl, vp, cols, x, nr);
+      int sidx = 0;
+#pragma unroll 1
+      for (int j = 0; j < cl; ++j) {
+        cp_wait<D - 1>();  // this step's group has landed
+        __syncwarp();
+        const BStage<RPW>& S = ring[sidx];
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) {
+          const double2 xv = *reinterpret_cast<const double2*>(&S.xs[lane][comp][0]);
+          const double m0 = S.v[comp][rl], m1 = S.v[3 + comp][rl], m2 = S.v[6 + comp][rl];
+          acc[0][0] += m0 * xv.x;
+          acc[0][1] += m0 * xv.y;
+          acc[1][0] += m1 * xv.x;
+          acc[1][1] += m1 * xv.y;
+          acc[2][0] += m2 * xv.x;
+          acc[2][1] += m2 * xv.y;
+        }
+        __syncwarp();  // every lane is done with the stage before it is refilled
+        bstage_issue<RPW>(ring[sidx], lane, rl, k0, j + D, cl, vp, cols, x, nr);
+        sidx = sidx + 1 == D ? 0 : sidx + 1;
+      }
+      cp_wait<0>();
+      __syncwarp();  // the ring and the columns are free for the next chunk or task
+    }
+    if (row < N) {
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        st_g<2>(y + (3 * row + r) * nr + k0, acc[r]);
+        if (MODE == 1) {
+          double xr[2];
+          ldg_g<2>(x + (3 * row + r) * nr + k0, xr);
+          dot[0][0] += xr[0] * acc[r][0];
+          dot[0][1] += xr[1] * acc[r][1];
+        }
+      }
+    }
+  }
+  if (MODE == 1) {
+    double tot[1];
+    if (rhs_grid_sum<2, 1>(dot, TPR, nr, partials, &s->ticket[0], tot)) {
+      const int kk = threadIdx.x;
+      const bool ok = s->active[kk] && fabs(tot[0]) > 1e-300 && isfinite(tot[0]);
+      s->alpha[kk] = ok ? s->rz[kk] / tot[0] : 0.0;
+      if (s->active[kk] && !ok) s->active[kk] = 0;  // breakdown of this rhs
+    }
+  }
+}
+
 // x += alpha p, r -= alpha q, then r.z and r.r per rhs, beta and the stop tests.
 template <int G>
 __global__ void __launch_bounds__(kBlk)
@@ -398,9 +559,53 @@ struct BlockRun {
   int g_spmv, g_vec;
 };
 
+template <int RPW>
+void launch_bspmv_pipe(const BlockRun& B, cudaStream_t st, int mode, const double* x, double* y) {
+  Ctx* c = B.c;
+  constexpr size_t sm = bpipe_smem<RPW>();
+  if (mode == 1)
+    k_bspmv_pipe<RPW, 1><<<B.g_spmv, kBlk, sm, st>>>(c->N, c->nslices, c->slice_ptr, c->sell_col, c->val64, x, y,
+                                                      B.nr, B.s, B.partials);
+  else
+    k_bspmv_pipe<RPW, 0><<<B.g_spmv, kBlk, sm, st>>>(c->N, c->nslices, c->slice_ptr, c->sell_col, c->val64, x, y,
+                                                      B.nr, B.s, B.partials);
+}
+
+// The pipelined kernels use more than the default 48 KB of dynamic shared
+// memory; the limit is raised for the current device before any launch (and
+// before any graph capture).
+template <int RPW>
+cudaError_t bpipe_attr() {
+  constexpr int sm = (int)bpipe_smem<RPW>();
+  cudaError_t e = cudaFuncSetAttribute(k_bspmv_pipe<RPW, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_bspmv_pipe<RPW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  return e;
+}
+
+cudaError_t prepare_bspmv(int tpr) {
+  switch (tpr) {
+    case 2: return bpipe_attr<16>();
+    case 4: return bpipe_attr<8>();
+    case 8: return bpipe_attr<4>();
+    case 16: return bpipe_attr<2>();
+    default: return cudaSuccess;
+  }
+}
+
 template <int G>
 void launch_bspmv(const BlockRun& B, cudaStream_t st, int mode, const double* x, double* y) {
   Ctx* c = B.c;
+  if constexpr (G == 2) {
+    // 4..32 right-hand sides: the pipelined kernel (rows per warp task = 32 / tpr)
+    switch (B.tpr) {
+      case 2: launch_bspmv_pipe<16>(B, st, mode, x, y); return;
+      case 4: launch_bspmv_pipe<8>(B, st, mode, x, y); return;
+      case 8: launch_bspmv_pipe<4>(B, st, mode, x, y); return;
+      case 16: launch_bspmv_pipe<2>(B, st, mode, x, y); return;
+      default: break;
+    }
+  }
   if (mode == 1)
     k_bspmv<G, 1><<<B.g_spmv, kBlk, 0, st>>>(c->N, c->nslices, c->slice_ptr, c->sell_col, c->val64, x, y, B.nr,
                                               B.tpr, B.s, B.partials);
@@ -534,6 +739,7 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* Bm, double* X, const ufc_sol
   B.nn = c->n * nr;
   B.dinv = algo->precond_type == UFC_SOLV_PREC_JACOBI ? c->dinv64 : nullptr;
   B.g_spmv = grid_blocks(c->nslices * B.tpr * 32);
+  if (G == 2) UFC_CUDA(c, prepare_bspmv(B.tpr));
   B.g_vec = grid_blocks(c->n * B.tpr);
   BScalars* hs = nullptr;
   int32_t* restart_dev = nullptr;
