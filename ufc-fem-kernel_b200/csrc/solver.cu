@@ -363,6 +363,93 @@ __global__ void __launch_bounds__(kSpmvBlock)
   }
 }
 
+// The symmetric product with SPLIT warps per slice for meshes with too few
+// slices to fill the GPU one warp each: warp `part` of a slice takes the
+// upper and lower steps j = part, part + SPLIT, ..., and the row sums of the
+// slice's warps are added in shared memory in warp order.
+template <typename TV, typename TX, typename TA, int MODE, int SPLIT>
+__global__ void __launch_bounds__(kSpmvBlock)
+    k_spmv_sym_split(int32_t N, int64_t nslices, const int64_t* __restrict__ uptr, const int32_t* __restrict__ ucol,
+                     const int64_t* __restrict__ lptr, const int32_t* __restrict__ lpos,
+                     const int32_t* __restrict__ lcol, const TV* __restrict__ val, const TX* __restrict__ x,
+                     TX* __restrict__ y, CgScalars* __restrict__ scal, double* __restrict__ partials) {
+  if (MODE == kCg && scal->stop) return;
+  constexpr int kWarps = kSpmvBlock / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int part = warp % SPLIT;
+  const int64_t s = (int64_t)blockIdx.x * (kWarps / SPLIT) + warp / SPLIT;
+  const int64_t row = s * kSlice + lane;
+  TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
+  if (s < nslices) {
+    const int64_t ub = uptr[s], lb = lptr[s];
+    const int ulen = (int)((uptr[s + 1] - ub) >> 5);
+    const int llen = (int)((lptr[s + 1] - lb) >> 5);
+    const int32_t* ucp = ucol + ub + lane;
+    const TV* uvp = val + 9 * ub + lane;
+    const int32_t* lpp = lpos + lb + lane;
+    const int32_t* lcp = lcol + lb + lane;
+    auto upper = [&](int j) {
+      const int64_t cj = __ldcs(ucp + 32 * j);
+      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
+      const TV* v = uvp + 288 * (int64_t)j;
+      a0 += (TA)v[0] * x0 + (TA)v[32] * x1 + (TA)v[64] * x2;
+      a1 += (TA)v[96] * x0 + (TA)v[128] * x1 + (TA)v[160] * x2;
+      a2 += (TA)v[192] * x0 + (TA)v[224] * x1 + (TA)v[256] * x2;
+    };
+    auto lower = [&](int j) {
+      const int64_t P = __ldcs(lpp + 32 * j);
+      const int64_t cj = __ldcs(lcp + 32 * j);
+      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
+      const TV* v = val + 9 * (P & ~int64_t(31)) + (P & 31);
+      a0 += (TA)__ldg(v) * x0 + (TA)__ldg(v + 96) * x1 + (TA)__ldg(v + 192) * x2;
+      a1 += (TA)__ldg(v + 32) * x0 + (TA)__ldg(v + 128) * x1 + (TA)__ldg(v + 224) * x2;
+      a2 += (TA)__ldg(v + 64) * x0 + (TA)__ldg(v + 160) * x1 + (TA)__ldg(v + 256) * x2;
+    };
+    const int mlen = ulen < llen ? ulen : llen;
+    int j = part;
+#pragma unroll 1
+    for (; j < mlen; j += SPLIT) {
+      upper(j);
+      lower(j);
+    }
+    for (int k = j; k < ulen; k += SPLIT) upper(k);
+    for (int k = j; k < llen; k += SPLIT) lower(k);
+  }
+  {
+    __shared__ TA sh[kWarps][3][32];
+    sh[warp][0][lane] = a0;
+    sh[warp][1][lane] = a1;
+    sh[warp][2][lane] = a2;
+    __syncthreads();
+    if (part == 0) {
+#pragma unroll
+      for (int q = 1; q < SPLIT; ++q) {
+        a0 += sh[warp + q][0][lane];
+        a1 += sh[warp + q][1][lane];
+        a2 += sh[warp + q][2][lane];
+      }
+    }
+  }
+  double dot[1] = {0.0};
+  if (part == 0 && s < nslices && row < N) {
+    y[3 * row] = (TX)a0;
+    y[3 * row + 1] = (TX)a1;
+    y[3 * row + 2] = (TX)a2;
+    if (MODE == kCg) dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
+  }
+  if (MODE == kCg) {
+    double tot[1];
+    if (grid_sum<1>(dot, partials, &scal->ticket[0], tot)) {
+      scal->pq = tot[0];
+      if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
+        scal->stop = 3;
+      } else {
+        scal->alpha = scal->rz / tot[0];
+      }
+    }
+  }
+}
+
 // 4 consecutive entries through 16-byte loads and stores (cudaMalloc bases are
 // 256-byte aligned; callers pass offsets that are multiples of 4 entries).
 template <typename T>
@@ -551,10 +638,27 @@ Vecs<TV, TX> vecs(Ctx* c, bool precond) {
   return v;
 }
 
+template <typename TV, typename TX, typename TA, int MODE, int SPLIT>
+void launch_spmv_sym_split(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
+  constexpr int per_block = kSpmvBlock / 32 / SPLIT;
+  const int grid = (int)((c->nslices + per_block - 1) / per_block);
+  k_spmv_sym_split<TV, TX, TA, MODE, SPLIT><<<grid, kSpmvBlock, 0, st>>>(
+      c->N, c->nslices, c->uptr, c->ucol, c->lptr, c->lpos, c->lcol, val, x, y, c->scal, c->partials);
+}
+
+// The symmetric product: one warp per slice (grid = slices / 8 blocks), or
+// SPLIT warps per slice on small meshes (the rule of spmv_split).
 template <typename TV, typename TX, typename TA, int MODE>
 void launch_spmv_sym(const Ctx* c, int grid, cudaStream_t st, const TV* val, const TX* x, TX* y) {
-  k_spmv_sym<TV, TX, TA, MODE><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->uptr, c->ucol, c->lptr,
-                                                            c->lpos, c->lcol, val, x, y, c->scal, c->partials);
+  switch (spmv_split(c)) {
+    case 1:
+      k_spmv_sym<TV, TX, TA, MODE><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->uptr, c->ucol, c->lptr,
+                                                                c->lpos, c->lcol, val, x, y, c->scal, c->partials);
+      break;
+    case 2: launch_spmv_sym_split<TV, TX, TA, MODE, 2>(c, st, val, x, y); break;
+    case 4: launch_spmv_sym_split<TV, TX, TA, MODE, 4>(c, st, val, x, y); break;
+    default: launch_spmv_sym_split<TV, TX, TA, MODE, 8>(c, st, val, x, y); break;
+  }
 }
 
 template <typename TV, typename TX, typename TA>
