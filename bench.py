@@ -176,27 +176,39 @@ def make_problem(args):
     return ufc, ufc.mesh.lognormal_cantilever(nx, ny, nz, seed=4)
 
 
-def cpu_sample(p, iters, reps=1, check=None):
+def cpu_sample(p, iters, reps=1, check=None, gpu_csr=None):
     """Oracle (CPU FP64, all host threads) per-iteration time of Jacobi-PCG on the
     problem's canonical CSR: setup time, seconds per iteration, threads, and for
     each GPU solution in `check` (name -> host array) its relative residual
-    ||b - K u|| / ||b|| with the oracle's own assembly and right-hand side."""
+    ||b - K u|| / ||b|| with the oracle's own assembly and right-hand side.
+    gpu_csr, when given, returns the GPU's exported canonical CSR (row_ptr, col,
+    FP64 values), compared with the oracle's: pattern equality and the largest
+    value difference relative to the largest entry (under "csr")."""
     from oracle import oracle as O
+
+    import numpy as np
 
     t0 = time.perf_counter()
     model = O.Model(p)
     K = model.assemble()
     b = model.lifted_rhs()
     setup = time.perf_counter() - t0
+    csr = None
+    if gpu_csr is not None:
+        rp, col, v = gpu_csr()
+        same = bool(np.array_equal(rp, K.row_ptr) and np.array_equal(col, K.col))
+        csr = {"pattern_equal": same, "nnz": int(col.size),
+               "values_rel_max_err": float(np.abs(v - K.val).max() / np.abs(K.val).max()) if same else None}
+        del rp, col, v
     per = []
     for _ in range(reps):
         t = time.perf_counter()
         O.pcg(K, b, max_iter=-iters)
         per.append((time.perf_counter() - t) / iters)
-    import numpy as np
-
     bn = float(np.linalg.norm(b))
     res = {k: float(np.linalg.norm(b - K.matvec(u)) / bn) for k, u in (check or {}).items()}
+    if csr is not None:
+        res["csr"] = csr
     return setup, per, O.num_threads(), res
 
 
@@ -337,6 +349,28 @@ def other_configs(ufc, local, stream):
         out["adjoint_128x64x64_16rhs"]["multigrid_iters_max"] = max(its)
         out["adjoint_128x64x64_16rhs"]["multigrid_vs_block_u_rel"] = (
             torch.linalg.vector_norm(Um - U) / torch.linalg.vector_norm(U)).item()
+        # dJ/drho of case 0's compliance J = f.u against central differences
+        # (h = 1e-6) on the 32 seeded elements; each difference is solved as a
+        # correction K' du = f - K' u0 with the multigrid PCG
+        g = model.fem.adjoint_sensitivity(U[:1].contiguous(), U[:1].contiguous()) * 3 * 210e3 * rho ** 2
+        h = 1e-6
+        f0 = F[0].contiguous()
+        worst = 0.0
+        for e in p.meta["fd_elems"]:
+            d = []
+            for sgn in (1.0, -1.0):
+                rp = rho.clone()
+                rp[int(e)] += sgn * h
+                model.set_moduli(210e3 * rp ** 3)
+                _, r, _, _ = model.fem.internal_force(U[0].contiguous(), f_ext=f0, update_state=False)
+                du, _ = model.fem.solve(r, mga)
+                d.append(torch.dot(f0, du).item())
+            fd = (d[0] - d[1]) / (2 * h)
+            worst = max(worst, abs(g[int(e)].item() - fd) / abs(fd))
+        model.set_moduli(210e3 * rho ** 3)
+        out["adjoint_128x64x64_16rhs"]["fd_check"] = {
+            "elements": len(p.meta["fd_elems"]), "h": h, "max_rel_err": worst,
+            "note": "adjoint dJ/drho of case 0's compliance (block solve) against central differences"}
         model.fem.close()
     except Exception as e:
         out["adjoint_128x64x64_16rhs"] = {"error": f"{type(e).__name__}: {e}"}
@@ -548,7 +582,8 @@ def run_ours(args):
         checks = {"fp32_refine": u_mixed.cpu().numpy(), "fp64": u_fp64.cpu().numpy()}
         if mg_line and "value" in mg_line:
             checks["multigrid"] = u_mg.cpu().numpy()
-        setup, per, threads, oracle_res = cpu_sample(p, args.cpu_iters, check=checks)
+        setup, per, threads, oracle_res = cpu_sample(p, args.cpu_iters, check=checks,
+                                                     gpu_csr=lambda: m.csr_export(index_base=0)[:3])
         iters64 = fst.niter
         cpu = {"value": per[0] * iters64, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{args.cpu_iters} FP64 Jacobi-PCG iterations of the oracle (OpenMP, canonical CSR) on "
@@ -597,8 +632,11 @@ def run_ours(args):
     }
     if oracle_res:
         # the GPU solutions checked with the oracle's CPU assembly of the same problem
+        csr = oracle_res.pop("csr", None)
         line["accuracy_vs_oracle"] = {"residual_rel": oracle_res,
                                       "note": "||b - K u|| / ||b|| with the oracle's canonical CSR and lifted b"}
+        if csr is not None:
+            line["accuracy_vs_oracle"]["csr"] = csr
     if other:
         line["other_storage"] = other
     if mg_line:
