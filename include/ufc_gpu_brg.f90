@@ -21,6 +21,17 @@ MODULE ufc_gpu_brg
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_PRECISION_FP64 = 0, UFC_PRECISION_FP32_REFINE = 1
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_BUILD_FP64 = 1, UFC_BUILD_FP32 = 2
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_BUILD_FP32_ROUNDED = 4, UFC_BUILD_FP32_DIFF = 8
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_BUILD_SYMMETRIC = 16
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_SOLV_PREC_NONE = 0, UFC_PRECISION_FP32_MATRIX = 2
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_ACCUMULATE_STORAGE = 0, UFC_ACCUMULATE_FP64 = 1
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_REFINE_KEEP_DIRECTION = 0, UFC_REFINE_RESTART = 1
+  ! IF_Err_Brg status codes (ufc_core/L1_IF/Error/IF_Err_Brg.f90:95-110)
+  INTEGER(C_INT), PARAMETER, PUBLIC :: UFC_STATUS_OK = 0, UFC_STATUS_INVALID = 1, UFC_STATUS_ERROR = 2
+  INTEGER(C_INT), PARAMETER, PUBLIC :: UFC_STATUS_CONVERGED = 3, UFC_STATUS_NOT_CONVERGED = 4
+  INTEGER(C_INT), PARAMETER, PUBLIC :: UFC_STATUS_NOT_FOUND = 5, UFC_STATUS_WARN = 6, UFC_STATUS_MEM_ERROR = 7
+  INTEGER(C_INT), PARAMETER, PUBLIC :: UFC_STATUS_IO_ERROR = 8, UFC_STATUS_EXISTS = 9, UFC_STATUS_FATAL = 10
+  INTEGER(C_INT), PARAMETER, PUBLIC :: UFC_STATUS_UNSUPPORTED = 11
+  INTEGER(C_INT64_T), PARAMETER, PUBLIC :: UFC_NOALLOC_MAX_ROWS = 16777216_C_INT64_T
 
   TYPE, BIND(C), PUBLIC :: ufc_mesh_desc
     INTEGER(C_INT32_T) :: n_nodes, n_elems
@@ -123,7 +134,18 @@ MODULE ufc_gpu_brg
     TYPE(C_PTR)           :: f
   END TYPE
 
+  TYPE, BIND(C), PUBLIC :: ufc_timing_info          ! device-time counters of the last solve
+    INTEGER(C_INT32_T) :: spmv_launches
+    REAL(C_DOUBLE)     :: spmv_ms
+    INTEGER(C_INT64_T) :: spmv_bytes
+    INTEGER(C_INT32_T) :: precision
+    INTEGER(C_INT64_T) :: kernel_launches
+  END TYPE
+
   PUBLIC :: ufc_ctx_create, ufc_ctx_destroy, ufc_last_error, ufc_mesh_set, ufc_material_set, ufc_bc_set
+  PUBLIC :: ufc_ctx_set_stream, ufc_ctx_set_instrument, ufc_stress_eval, ufc_spmv, ufc_mg_level_info
+  PUBLIC :: ufc_mg_export, ufc_last_timing, ufc_last_residual_history, ufc_set_displacement, ufc_get_state
+  PUBLIC :: ufc_csr_spmv_dot_noalloc
   PUBLIC :: ufc_pattern_build, ufc_csr_export, ufc_elem_compute_ke, ufc_elem_compute_fint
   PUBLIC :: ufc_mat_update_batch, ufc_pcg_solve, ufc_pcg_solve_block, ufc_nr_increment
   PUBLIC :: ufc_state_commit, ufc_state_rollback, ufc_get_displacement, ufc_adjoint_sensitivity
@@ -264,6 +286,70 @@ MODULE ufc_gpu_brg
       REAL(C_DOUBLE), INTENT(IN)    :: u(*), lam(*)
       REAL(C_DOUBLE), INTENT(OUT)   :: dJdE(*)
       INTEGER(C_INT32_T), VALUE     :: mem
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_ctx_set_stream(ctx, cuda_stream) BIND(C, NAME='ufc_ctx_set_stream')
+      IMPORT :: C_INT, C_PTR
+      TYPE(C_PTR), VALUE            :: ctx, cuda_stream   ! a cudaStream_t, or C_NULL_PTR for the context's own
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_ctx_set_instrument(ctx, on) BIND(C, NAME='ufc_ctx_set_instrument')
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx
+      INTEGER(C_INT32_T), VALUE     :: on
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_stress_eval(ctx, u, stress_gp, vm_gp, mem) BIND(C, NAME='ufc_stress_eval')
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx, u, stress_gp, vm_gp   ! C_NULL_PTR where not wanted
+      INTEGER(C_INT32_T), VALUE     :: mem
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_spmv(ctx, precision, x, y, mem) BIND(C, NAME='ufc_spmv')
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx, x, y          ! REAL(C_DOUBLE) or REAL(C_FLOAT) by precision
+      INTEGER(C_INT32_T), VALUE     :: precision, mem
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_mg_level_info(ctx, level, n_dof, nnz) BIND(C, NAME='ufc_mg_level_info')
+      IMPORT :: C_INT, C_PTR, C_INT32_T, C_INT64_T
+      TYPE(C_PTR), VALUE            :: ctx
+      INTEGER(C_INT32_T), VALUE     :: level
+      INTEGER(C_INT64_T), INTENT(OUT) :: n_dof, nnz
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_mg_export(ctx, level, arg) BIND(C, NAME='ufc_mg_export')
+      IMPORT :: C_INT, C_PTR, C_INT32_T, ufc_csr_export_arg
+      TYPE(C_PTR), VALUE                   :: ctx
+      INTEGER(C_INT32_T), VALUE            :: level
+      TYPE(ufc_csr_export_arg), INTENT(IN) :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_last_timing(ctx, info) BIND(C, NAME='ufc_last_timing')
+      IMPORT :: C_INT, C_PTR, ufc_timing_info
+      TYPE(C_PTR), VALUE                   :: ctx
+      TYPE(ufc_timing_info), INTENT(OUT)   :: info
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_last_residual_history(ctx, out, max_len, out_len) &
+        BIND(C, NAME='ufc_last_residual_history')
+      IMPORT :: C_INT, C_PTR, C_DOUBLE, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx
+      REAL(C_DOUBLE), INTENT(OUT)   :: out(*)
+      INTEGER(C_INT32_T), VALUE     :: max_len
+      INTEGER(C_INT32_T), INTENT(OUT) :: out_len
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_set_displacement(ctx, u, mem) BIND(C, NAME='ufc_set_displacement')
+      IMPORT :: C_INT, C_PTR, C_DOUBLE, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx
+      REAL(C_DOUBLE), INTENT(IN)    :: u(*)
+      INTEGER(C_INT32_T), VALUE     :: mem
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_get_state(ctx, eps_p_eq, stress, eps_p, mem) BIND(C, NAME='ufc_get_state')
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE            :: ctx, eps_p_eq, stress, eps_p   ! C_NULL_PTR where not wanted
+      INTEGER(C_INT32_T), VALUE     :: mem
+    END FUNCTION
+    ! device pointers (C_PTR from a CUDA Fortran or C allocation); no allocation inside
+    INTEGER(C_INT) FUNCTION ufc_csr_spmv_dot_noalloc(n_rows, row_ptr, col_ind, values, x, y, xy, cuda_stream, &
+        errbuf, errlen) BIND(C, NAME='ufc_csr_spmv_dot_noalloc')
+      IMPORT :: C_INT, C_PTR, C_INT64_T, C_INT32_T, C_CHAR
+      INTEGER(C_INT64_T), VALUE     :: n_rows
+      TYPE(C_PTR), VALUE            :: row_ptr, col_ind, values, x, y, xy, cuda_stream
+      CHARACTER(KIND=C_CHAR), INTENT(OUT) :: errbuf(*)
+      INTEGER(C_INT32_T), VALUE     :: errlen
     END FUNCTION
   END INTERFACE
 END MODULE ufc_gpu_brg

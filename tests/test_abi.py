@@ -74,3 +74,66 @@ def test_context_without_device_reports_status(pkg):
 def test_missing_library_fails_loudly(pkg, tmp_path):
     with pytest.raises(pkg.LibraryMissing):
         pkg._abi.load(str(tmp_path / "nope.so"))
+
+
+def _f90_types(text):
+    """Components (name, kind) of every TYPE, BIND(C) in the Fortran bridge, in order."""
+    import re
+
+    types, cur = {}, None
+    for raw in text.split("\n"):
+        line = raw.split("!")[0].strip()
+        m = re.match(r"TYPE,\s*BIND\(C\),\s*PUBLIC\s*::\s*(\w+)", line, re.I)
+        if m:
+            cur = m.group(1).lower()
+            types[cur] = []
+            continue
+        if cur and re.match(r"END\s+TYPE", line, re.I):
+            cur = None
+            continue
+        if cur and "::" in line:
+            kind, names = (part.strip() for part in line.split("::", 1))
+            names = re.sub(r"=\s*[^,]+", "", names)  # default initialisations
+            for nm in names.split(","):
+                nm = nm.strip()
+                dim = re.match(r"(\w+)\((\d+)\)", nm)
+                types[cur].append((dim.group(1) if dim else nm, kind.upper().replace(" ", ""),
+                                   int(dim.group(2)) if dim else 1))
+    return types
+
+
+def test_fortran_bridge_covers_the_header(pkg):
+    """include/ufc_gpu_brg.f90 (not compiled here: no Fortran compiler) binds
+    every function of the header, its BIND(C) types list the fields of the C
+    structs in order with matching kinds, and its constants have the header's
+    values."""
+    import re
+
+    A = pkg._abi
+    f90 = open(os.path.join(ROOT, "include", "ufc_gpu_brg.f90")).read()
+    header = open(os.path.join(ROOT, "include", "ufc_gpu.h")).read()
+    bound = {n.lower() for n in re.findall(r"BIND\(C,\s*NAME\s*=\s*'(ufc_\w+)'\)", f90, flags=re.I)}
+    assert set(A.header_functions()) <= bound, sorted(set(A.header_functions()) - bound)
+    kinds = {"INTEGER(C_INT32_T)": (C.c_int32,), "INTEGER(C_INT64_T)": (C.c_int64,),
+             "REAL(C_DOUBLE)": (C.c_double,), "TYPE(C_PTR)": (C.c_void_p,)}
+    types = _f90_types(f90)
+    for cname, pyname in STRUCTS.items():
+        assert cname in types, cname
+        fields = getattr(A, pyname)._fields_
+        comps = types[cname]
+        assert [c[0].lower() for c in comps] == [f[0].lower() for f in fields], cname
+        for (nm, kind, dim), (_, ctype) in zip(comps, fields):
+            if kind.startswith("TYPE(UFC_"):
+                assert ctype.__name__ == STRUCTS[kind[5:-1].lower()], (cname, nm)
+            elif dim > 1:
+                assert issubclass(ctype, C.Array) and ctype._length_ == dim, (cname, nm)
+            elif kind == "TYPE(C_PTR)":
+                assert ctype is C.c_void_p or issubclass(ctype, C._Pointer) or ctype in (C.c_char_p,), (cname, nm)
+            else:
+                assert C.sizeof(ctype) == C.sizeof(kinds[kind][0]) and (ctype in (C.c_double,)) == (
+                    kinds[kind][0] is C.c_double), (cname, nm, kind)
+    defines = dict(re.findall(r"#define (UFC_\w+) (-?\d+)", header))
+    params = re.findall(r"\b(UFC_\w+)\s*=\s*(-?\d+)", f90)
+    assert len(params) >= 30
+    for name, value in params:
+        assert name in defines and int(defines[name]) == int(value), name
