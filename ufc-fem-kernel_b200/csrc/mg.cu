@@ -60,6 +60,7 @@ struct MgLevel {
   double lmax = 0.0;
   double* inv = nullptr;     // coarsest level: dense inverse [n][n]
   float* inv32 = nullptr;
+  double *pv = nullptr, *pw = nullptr;  // power-iteration vectors (lambda_max), kept across refreshes
 };
 
 struct Mg {
@@ -69,6 +70,7 @@ struct Mg {
   bool stale = false;
   bool fp32 = false;         // the cycle runs in FP32 (values, vectors); the PCG around it in FP64
   int cheb_coarse = 0;       // degree of the coarsest Chebyshev solve (0: dense inverse)
+  double* dnorm = nullptr;   // ||v||^2 of the power iteration, on the device
 };
 
 namespace {
@@ -382,9 +384,11 @@ __global__ void k_mg_norm2(int64_t n, const double* __restrict__ v, double* __re
   if (grid_sum<1>(a, partials, ticket, tot)) *out = tot[0];
 }
 
-// v = D^-1 w / s
-__global__ void k_mg_scale_dinv(int64_t n, const double* __restrict__ w, const double* __restrict__ dinv, double s,
-                                double* __restrict__ v) {
+// v = D^-1 w / ||v_prev|| with ||v_prev||^2 read from the device (0: v = 0)
+__global__ void k_mg_scale_dinv(int64_t n, const double* __restrict__ w, const double* __restrict__ dinv,
+                                const double* __restrict__ nrm2, double* __restrict__ v) {
+  const double q = *nrm2;
+  const double s = q > 0.0 ? 1.0 / sqrt(q) : 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     v[i] = dinv[i] * w[i] * s;
 }
@@ -460,41 +464,29 @@ __global__ void k_mg_round(int64_t n, const double* __restrict__ a, float* __res
     b[i] = (float)a[i];
 }
 
-// lambda_max of D^-1 A on level L by power iteration (deterministic start), in FP64.
-int estimate_lmax(Ctx* owner, MgLevel& L, int iters) {
+// lambda_max of D^-1 A on level L by power iteration (deterministic start), in
+// FP64: v <- D^-1 A v / ||v||, lambda = ||v|| after the last step.  The norms
+// stay on the device, so the iterations run without a host round trip; the
+// vectors are kept for the next refresh.
+int estimate_lmax(Ctx* owner, Mg& mg, MgLevel& L, int iters) {
   Ctx* lc = L.c;
   const int64_t n = lc->n;
   const int g = grid_n(n);
-  double *v = nullptr, *w = nullptr, *dnorm = nullptr;
-  auto cleanup = [&]() {
-    dfree(&v);
-    dfree(&w);
-    dfree(&dnorm);
-  };
-  if (dalloc(owner, &v, n) != UFC_STATUS_OK || dalloc(owner, &w, n) != UFC_STATUS_OK ||
-      dalloc(owner, &dnorm, 1) != UFC_STATUS_OK) {
-    cleanup();
-    return UFC_STATUS_MEM_ERROR;
+  if (!L.pv) UFC_TRY(dalloc(owner, &L.pv, n));
+  if (!L.pw) UFC_TRY(dalloc(owner, &L.pw, n));
+  if (!mg.dnorm) UFC_TRY(dalloc(owner, &mg.dnorm, 1));
+  k_mg_start_vector<<<g, kBlk, 0, owner->stream>>>(n, lc->fixed, L.pv);
+  k_mg_norm2<<<g, kBlk, 0, owner->stream>>>(n, L.pv, owner->partials, &owner->scal->ticket[6], mg.dnorm);
+  for (int it = 0; it < iters; ++it) {
+    spmv64_on(lc, owner->stream, L.pv, L.pw);
+    k_mg_scale_dinv<<<g, kBlk, 0, owner->stream>>>(n, L.pw, lc->dinv64, mg.dnorm, L.pv);
+    k_mg_norm2<<<g, kBlk, 0, owner->stream>>>(n, L.pv, owner->partials, &owner->scal->ticket[6], mg.dnorm);
   }
-  k_mg_start_vector<<<g, kBlk, 0, owner->stream>>>(n, lc->fixed, v);
-  double lam = 0.0, nrm = 0.0;
-  k_mg_norm2<<<g, kBlk, 0, owner->stream>>>(n, v, owner->partials, &owner->scal->ticket[6], dnorm);
-  cudaMemcpyAsync(&nrm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, owner->stream);
-  cudaStreamSynchronize(owner->stream);
-  nrm = std::sqrt(nrm);
-  for (int it = 0; it < iters && nrm > 0.0; ++it) {
-    spmv64_on(lc, owner->stream, v, w);
-    k_mg_scale_dinv<<<g, kBlk, 0, owner->stream>>>(n, w, lc->dinv64, 1.0 / nrm, v);
-    k_mg_norm2<<<g, kBlk, 0, owner->stream>>>(n, v, owner->partials, &owner->scal->ticket[6], dnorm);
-    double q = 0.0;
-    cudaMemcpyAsync(&q, dnorm, sizeof(double), cudaMemcpyDeviceToHost, owner->stream);
-    cudaStreamSynchronize(owner->stream);
-    lam = std::sqrt(q);  // ||D^-1 A v|| / ||v|| with the previous v normalised
-    nrm = lam;
-  }
-  cleanup();
   UFC_CUDA(owner, cudaGetLastError());
-  L.lmax = lam;
+  double q = 0.0;
+  UFC_CUDA(owner, cudaMemcpyAsync(&q, mg.dnorm, sizeof(double), cudaMemcpyDeviceToHost, owner->stream));
+  UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
+  L.lmax = iters > 0 ? std::sqrt(q) : 0.0;
   return UFC_STATUS_OK;
 }
 
@@ -545,11 +537,11 @@ int dense_inverse(Ctx* owner, MgLevel& L, bool fp32) {
   }
   if (fp32) {
     std::vector<float> f(Inv.begin(), Inv.end());
-    UFC_TRY(dalloc(owner, &L.inv32, n * n));
+    if (!L.inv32) UFC_TRY(dalloc(owner, &L.inv32, n * n));  // same size at every refresh
     UFC_CUDA(owner, cudaMemcpyAsync(L.inv32, f.data(), sizeof(float) * n * n, cudaMemcpyHostToDevice, owner->stream));
     UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
   } else {
-    UFC_TRY(dalloc(owner, &L.inv, n * n));
+    if (!L.inv) UFC_TRY(dalloc(owner, &L.inv, n * n));
     UFC_CUDA(owner, cudaMemcpyAsync(L.inv, Inv.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice, owner->stream));
     UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
   }
@@ -570,6 +562,8 @@ void free_level(MgLevel& L) {
   dfree(&L.dinv32);
   dfree(&L.inv);
   dfree(&L.inv32);
+  dfree(&L.pv);
+  dfree(&L.pw);
   if (L.own_xb) {
     dfree(&L.x);
     dfree(&L.b);
@@ -674,6 +668,7 @@ void mg_mark_stale(Ctx* c) {
 void mg_free(Ctx* c) {
   if (!c->mg) return;
   for (auto& L : c->mg->lv) free_level(L);
+  dfree(&c->mg->dnorm);
   delete c->mg;
   c->mg = nullptr;
 }
@@ -755,11 +750,9 @@ int mg_numeric(Ctx* c) {
         UFC_TRY(mg_alloc(c, &L.b, n));
       }
     }
-    if (l + 1 < mg.lv.size() || n > kDenseMax) UFC_TRY(estimate_lmax(c, L, 15));
+    if (l + 1 < mg.lv.size() || n > kDenseMax) UFC_TRY(estimate_lmax(c, mg, L, 15));
   }
   MgLevel& Cst = mg.lv.back();
-  dfree(&Cst.inv);
-  dfree(&Cst.inv32);
   if (Cst.c->n <= kDenseMax) {
     UFC_TRY(dense_inverse(c, Cst, mg.fp32));
     mg.cheb_coarse = 0;
