@@ -61,7 +61,6 @@ struct MgLevel {
   double* inv = nullptr;     // coarsest level: dense inverse [n][n]
   float* inv32 = nullptr;
   double *pv = nullptr, *pw = nullptr;  // power-iteration vectors (lambda_max), kept across refreshes
-  double* gj = nullptr;      // coarsest level: the dense matrix, reduced in place by Gauss-Jordan
 };
 
 struct Mg {
@@ -72,7 +71,6 @@ struct Mg {
   bool fp32 = false;         // the cycle runs in FP32 (values, vectors); the PCG around it in FP64
   int cheb_coarse = 0;       // degree of the coarsest Chebyshev solve (0: dense inverse)
   double* dnorm = nullptr;   // ||v||^2 of the power iteration, on the device
-  int32_t* gj_err = nullptr; // singular coarsest matrix, set by the Gauss-Jordan kernel
 };
 
 namespace {
@@ -492,135 +490,61 @@ int estimate_lmax(Ctx* owner, Mg& mg, MgLevel& L, int iters) {
   return UFC_STATUS_OK;
 }
 
-// The dense coarsest matrix from its SELL storage: one thread per block row,
-// the canonical entries only (the SELL padding is skipped).  M is zeroed first.
-__global__ void k_mg_dense_fill(int32_t N, const int32_t* __restrict__ brow, const int32_t* __restrict__ bcol,
-                                const int64_t* __restrict__ sptr, const double* __restrict__ val, int64_t n,
-                                double* __restrict__ M) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  const int64_t b = brow[i], m = brow[i + 1] - b;
-  const int64_t s = i / kSlice, t = i % kSlice;
-  for (int64_t k = 0; k < m; ++k) {
-    const int64_t P = sptr[s] + k * kSlice + t;
-    const int64_t cb = bcol[b + k];
-    for (int r = 0; r < 3; ++r)
-      for (int cc = 0; cc < 3; ++cc) M[(3 * i + r) * n + 3 * cb + cc] = val[vpos(P, r * 3 + cc)];
-  }
-}
-
-constexpr int kGjThreads = 1024;
-
-// Inv = M^-1 by Gauss-Jordan elimination with partial pivoting, one block of
-// 1024 threads, M reduced in place (n <= kDenseMax, both n x n in global
-// memory, L2-resident).  Column c: the pivot is the first row i >= c of largest
-// |M[i][c]|; rows c and pivot swap; row c is scaled by 1 / M[c][c]; every other
-// row i with f = M[i][c] != 0 takes M[i][:] -= f M[c][:] (products and
-// differences rounded separately, no fused multiply-add).  A zero pivot sets
-// *err and ends the kernel.
-__global__ void __launch_bounds__(kGjThreads)
-    k_mg_gauss_jordan(int n, double* __restrict__ M, double* __restrict__ Inv, int32_t* __restrict__ err) {
-  __shared__ double f[kDenseMax];
-  __shared__ double wv[kGjThreads / 32];
-  __shared__ int wi[kGjThreads / 32];
-  __shared__ double best_s;
-  __shared__ int piv_s;
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
-  for (int i = w; i < n; i += nw)
-    for (int j = lane; j < n; j += 32) Inv[(int64_t)i * n + j] = i == j ? 1.0 : 0.0;
-  __syncthreads();
-  for (int c = 0; c < n; ++c) {
-    double bv = -1.0;
-    int bi = n;
-    for (int i = c + tid; i < n; i += blockDim.x) {
-      const double a = fabs(M[(int64_t)i * n + c]);
-      if (a > bv) {
-        bv = a;
-        bi = i;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_down_sync(0xffffffffu, bv, o);
-      const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-      if (ov > bv || (ov == bv && oi < bi)) {
-        bv = ov;
-        bi = oi;
-      }
-    }
-    if (lane == 0) {
-      wv[w] = bv;
-      wi[w] = bi;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      double v = wv[0];
-      int ix = wi[0];
-      for (int k = 1; k < nw; ++k)
-        if (wv[k] > v || (wv[k] == v && wi[k] < ix)) {
-          v = wv[k];
-          ix = wi[k];
-        }
-      best_s = v;
-      piv_s = ix;
-    }
-    __syncthreads();
-    if (!(best_s > 0.0)) {
-      if (tid == 0) *err = 1;
-      return;
-    }
-    const int piv = piv_s;
-    if (piv != c) {
-      for (int j = tid; j < n; j += blockDim.x) {
-        const double m0 = M[(int64_t)c * n + j], i0 = Inv[(int64_t)c * n + j];
-        M[(int64_t)c * n + j] = M[(int64_t)piv * n + j];
-        Inv[(int64_t)c * n + j] = Inv[(int64_t)piv * n + j];
-        M[(int64_t)piv * n + j] = m0;
-        Inv[(int64_t)piv * n + j] = i0;
-      }
-      __syncthreads();
-    }
-    const double sc = 1.0 / M[(int64_t)c * n + c];
-    __syncthreads();  // every thread has read the pivot before row c is scaled
-    for (int j = tid; j < n; j += blockDim.x) {
-      M[(int64_t)c * n + j] = __dmul_rn(M[(int64_t)c * n + j], sc);
-      Inv[(int64_t)c * n + j] = __dmul_rn(Inv[(int64_t)c * n + j], sc);
-    }
-    for (int i = tid; i < n; i += blockDim.x) f[i] = i == c ? 0.0 : M[(int64_t)i * n + c];
-    __syncthreads();
-    for (int i = w; i < n; i += nw) {
-      const double fi = f[i];
-      if (fi == 0.0) continue;
-      for (int j = lane; j < n; j += 32) {
-        M[(int64_t)i * n + j] = __dsub_rn(M[(int64_t)i * n + j], __dmul_rn(fi, M[(int64_t)c * n + j]));
-        Inv[(int64_t)i * n + j] = __dsub_rn(Inv[(int64_t)i * n + j], __dmul_rn(fi, Inv[(int64_t)c * n + j]));
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Dense inverse of the coarsest matrix on the device (FP64, rounded to FP32
-// for an FP32 cycle); the buffers are kept across refreshes.
-int dense_inverse(Ctx* owner, Mg& mg, MgLevel& L, bool fp32) {
+// Dense inverse of the coarsest matrix (Gauss-Jordan with partial pivoting).
+int dense_inverse(Ctx* owner, MgLevel& L, bool fp32) {
   Ctx* lc = L.c;
-  const int64_t n = lc->n;
-  if (n > kDenseMax) return fail(owner, UFC_STATUS_INVALID, "multigrid: coarsest level too large for a dense inverse");
-  if (!L.gj) UFC_TRY(dalloc(owner, &L.gj, n * n));
-  if (!L.inv) UFC_TRY(dalloc(owner, &L.inv, n * n));
-  if (fp32 && !L.inv32) UFC_TRY(dalloc(owner, &L.inv32, n * n));
-  if (!mg.gj_err) UFC_TRY(dalloc(owner, &mg.gj_err, 1));
-  UFC_CUDA(owner, cudaMemsetAsync(L.gj, 0, sizeof(double) * n * n, owner->stream));
-  UFC_CUDA(owner, cudaMemsetAsync(mg.gj_err, 0, sizeof(int32_t), owner->stream));
-  k_mg_dense_fill<<<grid_for(lc->N, 128), 128, 0, owner->stream>>>(lc->N, lc->brow, lc->bcol, lc->slice_ptr,
-                                                                   lc->val64, n, L.gj);
-  k_mg_gauss_jordan<<<1, kGjThreads, 0, owner->stream>>>((int)n, L.gj, L.inv, mg.gj_err);
-  if (fp32) k_mg_round<<<grid_n(n * n), kBlk, 0, owner->stream>>>(n * n, L.inv, L.inv32);
-  UFC_CUDA(owner, cudaGetLastError());
-  owner->launches += fp32 ? 3 : 2;
-  int32_t e = 0;
-  UFC_CUDA(owner, cudaMemcpyAsync(&e, mg.gj_err, sizeof(int32_t), cudaMemcpyDeviceToHost, owner->stream));
-  UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
-  if (e) return fail(owner, UFC_STATUS_ERROR, "ufc_mg_setup: singular coarsest matrix (unconstrained rigid modes?)");
+  const int64_t n = lc->n, nnz = 9 * lc->nnzb;
+  std::vector<int64_t> rp(n + 1);
+  std::vector<int32_t> col(nnz);
+  std::vector<double> val(nnz);
+  ufc_csr_export_arg a{};
+  a.index_base = 0;
+  a.mem = UFC_MEM_HOST;
+  a.row_ptr = rp.data();
+  a.col_ind = col.data();
+  a.values = val.data();
+  UFC_TRY(export_csr(lc, &a));
+  std::vector<double> M((size_t)n * n, 0.0), Inv((size_t)n * n, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) M[i * n + col[k]] = val[k];
+    Inv[i * n + i] = 1.0;
+  }
+  for (int64_t c = 0; c < n; ++c) {
+    int64_t piv = c;
+    for (int64_t i = c + 1; i < n; ++i)
+      if (std::fabs(M[i * n + c]) > std::fabs(M[piv * n + c])) piv = i;
+    if (!(std::fabs(M[piv * n + c]) > 0.0))
+      return fail(owner, UFC_STATUS_ERROR, "ufc_mg_setup: singular coarsest matrix (unconstrained rigid modes?)");
+    if (piv != c)
+      for (int64_t j = 0; j < n; ++j) {
+        std::swap(M[c * n + j], M[piv * n + j]);
+        std::swap(Inv[c * n + j], Inv[piv * n + j]);
+      }
+    const double s = 1.0 / M[c * n + c];
+    for (int64_t j = 0; j < n; ++j) {
+      M[c * n + j] *= s;
+      Inv[c * n + j] *= s;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      if (i == c) continue;
+      const double f = M[i * n + c];
+      if (f == 0.0) continue;
+      for (int64_t j = 0; j < n; ++j) {
+        M[i * n + j] -= f * M[c * n + j];
+        Inv[i * n + j] -= f * Inv[c * n + j];
+      }
+    }
+  }
+  if (fp32) {
+    std::vector<float> f(Inv.begin(), Inv.end());
+    if (!L.inv32) UFC_TRY(dalloc(owner, &L.inv32, n * n));  // same size at every refresh
+    UFC_CUDA(owner, cudaMemcpyAsync(L.inv32, f.data(), sizeof(float) * n * n, cudaMemcpyHostToDevice, owner->stream));
+    UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
+  } else {
+    if (!L.inv) UFC_TRY(dalloc(owner, &L.inv, n * n));
+    UFC_CUDA(owner, cudaMemcpyAsync(L.inv, Inv.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice, owner->stream));
+    UFC_CUDA(owner, cudaStreamSynchronize(owner->stream));
+  }
   return UFC_STATUS_OK;
 }
 
@@ -640,7 +564,6 @@ void free_level(MgLevel& L) {
   dfree(&L.inv32);
   dfree(&L.pv);
   dfree(&L.pw);
-  dfree(&L.gj);
   if (L.own_xb) {
     dfree(&L.x);
     dfree(&L.b);
@@ -746,7 +669,6 @@ void mg_free(Ctx* c) {
   if (!c->mg) return;
   for (auto& L : c->mg->lv) free_level(L);
   dfree(&c->mg->dnorm);
-  dfree(&c->mg->gj_err);
   delete c->mg;
   c->mg = nullptr;
 }
@@ -832,7 +754,7 @@ int mg_numeric(Ctx* c) {
   }
   MgLevel& Cst = mg.lv.back();
   if (Cst.c->n <= kDenseMax) {
-    UFC_TRY(dense_inverse(c, mg, Cst, mg.fp32));
+    UFC_TRY(dense_inverse(c, Cst, mg.fp32));
     mg.cheb_coarse = 0;
   } else {
     mg.cheb_coarse = 24;
