@@ -44,6 +44,17 @@ WORKLOAD = ("C3D8 cantilever 192x96x96 unit hexes (1,769,472 elements, 5,447,811
             "Jacobi-PCG from x0=0 to ||f-Ku||/||f|| <= 1e-10 (FP64 residual)")
 
 
+def workload(mesh):
+    """The workload text of a --mesh other than the 192x96x96 default."""
+    if mesh == "192x96x96":
+        return WORKLOAD
+    nx, ny, nz = mesh_dims(mesh)
+    n_dof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    return (f"C3D8 cantilever {mesh} unit hexes ({nx * ny * nz:,} elements, {n_dof:,} DOF), lognormal E "
+            f"(mu ln 210e3, sigma 0.5, seed 4), nu 0.3, clamped x=0, traction (0,0,-1) on x={nx}; Jacobi-PCG from "
+            "x0=0 to ||f-Ku||/||f|| <= 1e-10 (FP64 residual)")
+
+
 def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -408,7 +419,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, numpy)",
-            "config": {"workload": WORKLOAD, "parallelism": "host threads", "l2": "n/a (CPU)"},
+            "config": {"workload": workload(args.mesh), "parallelism": "host threads", "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{args.cpu_iters} FP64 Jacobi-PCG iterations per step on the canonical "
                                        f"CSR (oracle, OpenMP), median s/iter x {FP64_ITERS_192x96x96} iterations; "
@@ -596,7 +607,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (matrix, CG vectors, SpMV rows) + f64 (solution, residual replacement)",
         "data": "synthetic (seeded numpy mesh and moduli)",
-        "config": {"workload": WORKLOAD, "mesh": args.mesh, "n_dof": info["n_dof"], "nnz": info["nnz"],
+        "config": {"workload": workload(args.mesh), "mesh": args.mesh, "n_dof": info["n_dof"], "nnz": info["nnz"],
                    "nnzb": info["nnzb"], "sell_blocks": info["sell_blocks"],
                    "parallelism": "replicas" if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (FP32 matrix 1.23 GB symmetric / 1.93 GB full per SpMV)",
