@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <utility>
 
 #include "c3d8_device.cuh"
 #include "reduce.cuh"
@@ -35,6 +36,50 @@ namespace {
 
 constexpr int kSpmvBlock = 256;
 constexpr int kVecBlock = 256;
+
+#ifndef UFC_PDL
+#define UFC_PDL 1
+#endif
+
+// Programmatic dependent launch between the kernels of a CG iteration: each
+// kernel lets its successor launch as soon as all of its own blocks are
+// running (launch_dependents), and waits for its predecessor's completion and
+// memory (wait) before it reads anything; both are no-ops for a kernel
+// launched without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+#if UFC_PDL
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" :::);
+#endif
+}
+
+template <typename... K, typename... A>
+void launch_pdl(void (*kernel)(K...), int grid, int block, cudaStream_t st, A&&... args) {
+#if UFC_PDL
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+#else
+  kernel<<<grid, block, 0, st>>>(std::forward<A>(args)...);
+#endif
+}
+
+// The CG variants of the products (MODE kCg) run inside the iteration chain.
+template <int MODE, typename... K, typename... A>
+void launch_mode(void (*kernel)(K...), int grid, int block, cudaStream_t st, A&&... args) {
+  if constexpr (MODE == 1)
+    launch_pdl(kernel, grid, block, st, std::forward<A>(args)...);
+  else
+    kernel<<<grid, block, 0, st>>>(std::forward<A>(args)...);
+}
 
 int vec_grid(int64_t n) {
   int dev = 0, sms = 148;
@@ -55,6 +100,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
     k_spmv(int32_t N, int64_t nrows_pad, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
            const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y, CgScalars* __restrict__ scal,
            double* __restrict__ partials) {
+  pdl_enter();
   if (MODE == kCg && scal->stop) return;
   const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
   double dot[1] = {0.0};
@@ -118,6 +164,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
     k_spmv_split(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
            const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y, CgScalars* __restrict__ scal,
            double* __restrict__ partials) {
+  pdl_enter();
   if (MODE == kCg && scal->stop) return;
   constexpr int kWarps = kSpmvBlock / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -205,13 +252,13 @@ template <typename TV, typename TX, typename TA, int MODE, bool DIFF, int SPLIT>
 void launch_spmv_split(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
   if constexpr (SPLIT == 1) {
     const int grid = (int)((c->nslices * kSlice + kSpmvBlock - 1) / kSpmvBlock);
-    k_spmv<TV, TX, TA, MODE, DIFF><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->slice_ptr,
-                                                                c->sell_col, val, x, y, c->scal, c->partials);
+    launch_mode<MODE>(k_spmv<TV, TX, TA, MODE, DIFF>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice,
+                      c->slice_ptr, c->sell_col, val, x, y, c->scal, c->partials);
   } else {
     constexpr int per_block = kSpmvBlock / 32 / SPLIT;
     const int grid = (int)((c->nslices + per_block - 1) / per_block);
-    k_spmv_split<TV, TX, TA, MODE, DIFF, SPLIT><<<grid, kSpmvBlock, 0, st>>>(
-        c->N, c->nslices, c->slice_ptr, c->sell_col, val, x, y, c->scal, c->partials);
+    launch_mode<MODE>(k_spmv_split<TV, TX, TA, MODE, DIFF, SPLIT>, grid, kSpmvBlock, st, c->N, c->nslices,
+                      c->slice_ptr, c->sell_col, val, x, y, c->scal, c->partials);
   }
 }
 
@@ -274,6 +321,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
                const int64_t* __restrict__ lptr, const int32_t* __restrict__ lpos, const int32_t* __restrict__ lcol,
                const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y,
                CgScalars* __restrict__ scal, double* __restrict__ partials) {
+  pdl_enter();
   if (MODE == kCg && scal->stop) return;
   const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
   double dot[1] = {0.0};
@@ -373,6 +421,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
                      const int64_t* __restrict__ lptr, const int32_t* __restrict__ lpos,
                      const int32_t* __restrict__ lcol, const TV* __restrict__ val, const TX* __restrict__ x,
                      TX* __restrict__ y, CgScalars* __restrict__ scal, double* __restrict__ partials) {
+  pdl_enter();
   if (MODE == kCg && scal->stop) return;
   constexpr int kWarps = kSpmvBlock / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -478,6 +527,7 @@ __global__ void __launch_bounds__(kVecBlock)
     k_cg_update(int64_t n, const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ r,
                 double* __restrict__ x, const T* __restrict__ dinv, CgScalars* __restrict__ scal,
                 double* __restrict__ partials) {
+  pdl_enter();
   if (scal->stop) return;
   const double alpha = scal->alpha;
   const T a = (T)alpha;
@@ -534,6 +584,7 @@ template <typename T>
 __global__ void __launch_bounds__(kVecBlock)
     k_cg_pupdate(int64_t n, const T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ p,
                  const CgScalars* __restrict__ scal) {
+  pdl_enter();
   if (scal->stop) return;
   const T beta = (T)scal->beta;
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
@@ -642,8 +693,8 @@ template <typename TV, typename TX, typename TA, int MODE, int SPLIT>
 void launch_spmv_sym_split(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
   constexpr int per_block = kSpmvBlock / 32 / SPLIT;
   const int grid = (int)((c->nslices + per_block - 1) / per_block);
-  k_spmv_sym_split<TV, TX, TA, MODE, SPLIT><<<grid, kSpmvBlock, 0, st>>>(
-      c->N, c->nslices, c->uptr, c->ucol, c->lptr, c->lpos, c->lcol, val, x, y, c->scal, c->partials);
+  launch_mode<MODE>(k_spmv_sym_split<TV, TX, TA, MODE, SPLIT>, grid, kSpmvBlock, st, c->N, c->nslices, c->uptr,
+                    c->ucol, c->lptr, c->lpos, c->lcol, val, x, y, c->scal, c->partials);
 }
 
 // The symmetric product: one warp per slice (grid = slices / 8 blocks), or
@@ -652,8 +703,8 @@ template <typename TV, typename TX, typename TA, int MODE>
 void launch_spmv_sym(const Ctx* c, int grid, cudaStream_t st, const TV* val, const TX* x, TX* y) {
   switch (spmv_split(c)) {
     case 1:
-      k_spmv_sym<TV, TX, TA, MODE><<<grid, kSpmvBlock, 0, st>>>(c->N, c->nslices * kSlice, c->uptr, c->ucol, c->lptr,
-                                                                c->lpos, c->lcol, val, x, y, c->scal, c->partials);
+      launch_mode<MODE>(k_spmv_sym<TV, TX, TA, MODE>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice, c->uptr,
+                        c->ucol, c->lptr, c->lpos, c->lcol, val, x, y, c->scal, c->partials);
       break;
     case 2: launch_spmv_sym_split<TV, TX, TA, MODE, 2>(c, st, val, x, y); break;
     case 4: launch_spmv_sym_split<TV, TX, TA, MODE, 4>(c, st, val, x, y); break;
@@ -670,8 +721,8 @@ void launch_iteration(const Run& R, const Vecs<TV, TX>& V, cudaStream_t st, cuda
   else
     launch_spmv<TV, TX, TA, kCg>(c, st, V.val, V.p, V.q);
   if (ev1) cudaEventRecord(ev1, st);
-  k_cg_update<TX><<<R.vg, kVecBlock, 0, st>>>(R.n, V.p, V.q, V.r, c->x64, V.dinv, c->scal, c->partials);
-  k_cg_pupdate<TX><<<R.vg, kVecBlock, 0, st>>>(R.n, V.r, V.dinv, V.p, c->scal);
+  launch_pdl(k_cg_update<TX>, R.vg, kVecBlock, st, R.n, V.p, V.q, V.r, c->x64, V.dinv, c->scal, c->partials);
+  launch_pdl(k_cg_pupdate<TX>, R.vg, kVecBlock, st, R.n, V.r, V.dinv, V.p, c->scal);
   c->launches += 3;
 }
 
