@@ -37,25 +37,18 @@ namespace {
 constexpr int kSpmvBlock = 256;
 constexpr int kVecBlock = 256;
 
-#ifndef UFC_PDL
-#define UFC_PDL 1
-#endif
-
 // Programmatic dependent launch between the kernels of a CG iteration: each
 // kernel lets its successor launch as soon as all of its own blocks are
 // running (launch_dependents), and waits for its predecessor's completion and
 // memory (wait) before it reads anything; both are no-ops for a kernel
 // launched without the attribute.
 __device__ __forceinline__ void pdl_enter() {
-#if UFC_PDL
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" :::);
-#endif
 }
 
 template <typename... K, typename... A>
 void launch_pdl(void (*kernel)(K...), int grid, int block, cudaStream_t st, A&&... args) {
-#if UFC_PDL
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(block);
@@ -67,9 +60,6 @@ void launch_pdl(void (*kernel)(K...), int grid, int block, cudaStream_t st, A&&.
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
-#else
-  kernel<<<grid, block, 0, st>>>(std::forward<A>(args)...);
-#endif
 }
 
 // The CG variants of the products (MODE kCg) run inside the iteration chain.
