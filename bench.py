@@ -223,7 +223,31 @@ def cpu_sample(p, iters, reps=1, check=None, gpu_csr=None):
     return setup, per, O.num_threads(), res
 
 
-def linear_static(ufc, local, p):
+def cpu_linear(p, iters_gpu, full_max_dof=50000, sample_iters=12):
+    """The oracle's FP64 Jacobi-PCG (CPU, all host threads) on one linear-elastic
+    problem: the whole solve to rtol 1e-10 when the problem has at most
+    full_max_dof DOF, else sample_iters iterations extrapolated to the GPU's FP64
+    iteration count; the CSR assembly is timed on its own."""
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    model = O.Model(p)
+    K = model.assemble()
+    b = model.lifted_rhs()
+    t_asm = time.perf_counter() - t0
+    if p.n_dof <= full_max_dof:
+        t = time.perf_counter()
+        _, info = O.pcg(K, b, rtol=1e-10)
+        s, sample = time.perf_counter() - t, f"the whole solve ({info['iters']} iterations)"
+    else:
+        t = time.perf_counter()
+        O.pcg(K, b, max_iter=-sample_iters)
+        per = (time.perf_counter() - t) / sample_iters
+        s, sample = per * iters_gpu, f"{sample_iters} iterations, {per * 1e3:.1f} ms/iter x {iters_gpu} (GPU FP64 count)"
+    return {"s": s, "kind": "port", "cores": O.num_threads(), "assembly_s": t_asm, "sample": sample}
+
+
+def linear_static(ufc, local, p, cpu=False):
     """Time-to-rtol 1e-10 of one linear-elastic problem from x0 = 0: FP64
     Jacobi-PCG, the FP32+FP64-refined one (full storage) and FP64 PCG with the
     multigrid preconditioner, each timed by the library's CUDA events after one
@@ -255,10 +279,65 @@ def linear_static(ufc, local, p):
     res["multigrid"] = {"s": st.solve_time / 1e3, "iters": st.niter, "rnorm": st.rnorm, "converged": st.converged,
                         "levels": levels, "coarsest_dof": coarse, "setup_s": setup_ms / 1e3}
     m.close()
+    if cpu:
+        res["cpu_baseline"] = cpu_linear(p, res["fp64"]["iters"])
     return res
 
 
-def other_configs(ufc, local, stream):
+def cpu_j2(p, nr_iters, cg_iters, sample_iters=12):
+    """The oracle's cost of the J2 bar on the CPU (all host threads), from the
+    parts of one Newton iteration: the return map and internal force at every
+    Gauss point, the tangent assembly, and sample_iters FP64 Jacobi-PCG
+    iterations on that tangent, extrapolated to the GPU run's Newton and CG
+    iteration counts."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    model = O.Model(p)
+    G = model.E * 8
+    state = {"sig": np.zeros(G * 6), "epeq": np.zeros(G), "epl": np.zeros(G * 6)}
+    u = np.zeros(model.n)
+    t = time.perf_counter()
+    _, trial = model.fint_j2(u, u, state)
+    K = model.assemble(Dgp=trial["D"])
+    t_nr = time.perf_counter() - t
+    b = np.random.default_rng(0).standard_normal(model.n)  # any right-hand side: only the time is used
+    b[p.fixed] = 0.0
+    t = time.perf_counter()
+    O.pcg(K, b, max_iter=-sample_iters)
+    per = (time.perf_counter() - t) / sample_iters
+    return {"s": nr_iters * t_nr + cg_iters * per, "kind": "port", "cores": O.num_threads(),
+            "sample": f"one return map + tangent assembly ({t_nr:.3f} s) x {nr_iters} Newton iterations + "
+                      f"{sample_iters} PCG iterations ({per * 1e3:.2f} ms/iter) x {cg_iters}"}
+
+
+def cpu_adjoint(p, E, U, iters, sample_iters=12):
+    """The oracle's cost of the 16-case adjoint workload on the CPU (all host
+    threads): sample_iters FP64 Jacobi-PCG iterations on the density problem's
+    stiffness extrapolated to 16 solves of the GPU block's iteration count, plus
+    the sensitivity dJ/dE of all 16 cases timed in full."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    model = O.Model(p)
+    props = np.stack([E, p.props[:, 1]], axis=1)
+    K = model.assemble(props=props)
+    b = np.ascontiguousarray(U[0])
+    t = time.perf_counter()
+    O.pcg(K, b, max_iter=-sample_iters)
+    per = (time.perf_counter() - t) / sample_iters
+    t = time.perf_counter()
+    model.adjoint_dJdE(U, U, props=props)
+    t_sens = time.perf_counter() - t
+    n = U.shape[0]
+    return {"s": n * iters * per + t_sens, "kind": "port", "cores": O.num_threads(),
+            "sample": f"{sample_iters} PCG iterations ({per * 1e3:.1f} ms/iter) x {iters} x {n} cases + "
+                      f"the sensitivity of all {n} cases ({t_sens:.3f} s)"}
+
+
+def other_configs(ufc, local, stream, cpu=False):
     """The other device workloads of the path, timed with CUDA events: the
     40x8x8 cantilever and the 128x64x64 lognormal cantilever (linear static),
     the 64x32x32 J2 bar pulled to 1 % strain in 20 Newton-Raphson increments, and
@@ -270,7 +349,7 @@ def other_configs(ufc, local, stream):
     out = {}
     for key, make in (("cantilever_40x8x8", ufc.mesh.config1), ("lognormal_128x64x64", ufc.mesh.config2)):
         try:
-            out[key] = linear_static(ufc, local, make())
+            out[key] = linear_static(ufc, local, make(), cpu)
         except Exception as e:  # a failure here must not lose the headline line
             out[key] = {"error": f"{type(e).__name__}: {e}"}
     try:
@@ -317,6 +396,9 @@ def other_configs(ufc, local, stream):
             "s": t, "converged": ok, "nr_iterations": nr_iters,
             "pcg_iterations": lin_iters, "preconditioner": "geometric multigrid (FP64 V-cycle), numerics rebuilt "
                                                           "after every tangent assembly"}
+        if cpu:
+            out["j2_bar_64x32x32"]["cpu_baseline"] = cpu_j2(p, out["j2_bar_64x32x32"]["nr_iterations"],
+                                                           out["j2_bar_64x32x32"]["pcg_iterations"])
     except Exception as e:  # a failure here must not lose the headline line
         out["j2_bar_64x32x32"] = {"error": f"{type(e).__name__}: {e}"}
     try:
@@ -379,6 +461,9 @@ def other_configs(ufc, local, stream):
             fd = (d[0] - d[1]) / (2 * h)
             worst = max(worst, abs(g[int(e)].item() - fd) / abs(fd))
         model.set_moduli(210e3 * rho ** 3)
+        if cpu:
+            out["adjoint_128x64x64_16rhs"]["cpu_baseline"] = cpu_adjoint(
+                p, 210e3 * rho.cpu().numpy() ** 3, U.cpu().numpy(), max(s.niter for s in states))
         out["adjoint_128x64x64_16rhs"]["fd_check"] = {
             "elements": len(p.meta["fd_elems"]), "h": h, "max_rel_err": worst,
             "note": "adjoint dJ/drho of case 0's compliance (block solve) against central differences"}
@@ -656,7 +741,7 @@ def run_ours(args):
         line["cpu_baseline"] = cpu
     if not args.no_extras and world == 1:
         m.close()
-        line["other_configs"] = other_configs(ufc, local, stream)
+        line["other_configs"] = other_configs(ufc, local, stream, cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     m.close()
