@@ -515,8 +515,7 @@ int assemble(Ctx* c, int build, double* elapsed_ms) {
     return fail(c, UFC_STATUS_INVALID,
                 "ufc_elem_compute_ke: J2 tangent needs ufc_elem_compute_fint(update_state=1) first");
   UFC_TRY(ensure_pairs(c));
-  release_graphs(c);  // captured CG batches hold pointers to the values they read
-  mg_mark_stale(c);
+  mg_mark_stale(c);  // (cached CG graphs stay: they are keyed by the arrays and the SpMV form they read)
   cudaEvent_t e0, e1;
   UFC_CUDA(c, cudaEventCreate(&e0));
   UFC_CUDA(c, cudaEventCreate(&e1));
@@ -593,7 +592,6 @@ int assemble(Ctx* c, int build, double* elapsed_ms) {
     UFC_CUDA(c, cudaGetLastError());
     c->has_val32 = true;
     c->val32_diff = diff;
-    release_graphs(c);  // the SpMV form changed
   }
   if (sym) UFC_TRY(pack_symmetric(c, true, sym32));
   UFC_CUDA(c, cudaEventRecord(e1, c->stream));

@@ -763,8 +763,14 @@ int get_graph(const Run& R, const Vecs<TV, TX>& V, int batch, cudaGraphExec_t* o
   Ctx* c = R.c;
   // one cached graph per (value, vector, accumulator) type combination
   const int slot = sizeof(TV) == 8 ? 0 : sizeof(TX) == 8 ? 3 : sizeof(TA) == 8 ? 2 : 1;
-  const void* key = (const void*)V.dinv;  // graphs are rebuilt when buffers or the preconditioner change
-  if (c->cg_graph[slot] && c->cg_graph_batch[slot] == batch && c->cg_graph_key[slot] == key) {
+  // graphs are rebuilt when a buffer they read, the preconditioner, the storage
+  // (symmetric or full) or the FP32 SpMV form (difference or plain) changes; a
+  // reassembly into the same arrays keeps them
+  const void* key = (const void*)V.dinv;
+  const void* val = (const void*)V.val;
+  const int form = (V.sym ? 1 : 0) | (c->val32_diff ? 2 : 0);
+  if (c->cg_graph[slot] && c->cg_graph_batch[slot] == batch && c->cg_graph_key[slot] == key &&
+      c->cg_graph_val[slot] == val && c->cg_graph_form[slot] == form) {
     *out = c->cg_graph[slot];
     return UFC_STATUS_OK;
   }
@@ -782,6 +788,8 @@ int get_graph(const Run& R, const Vecs<TV, TX>& V, int batch, cudaGraphExec_t* o
   if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
   c->cg_graph_batch[slot] = batch;
   c->cg_graph_key[slot] = key;
+  c->cg_graph_val[slot] = val;
+  c->cg_graph_form[slot] = form;
   *out = c->cg_graph[slot];
   return UFC_STATUS_OK;
 }
@@ -1014,6 +1022,8 @@ void release_graphs(Ctx* c) {
     c->cg_graph[k] = nullptr;
     c->cg_graph_batch[k] = 0;
     c->cg_graph_key[k] = nullptr;
+    c->cg_graph_val[k] = nullptr;
+    c->cg_graph_form[k] = 0;
   }
 }
 

@@ -148,7 +148,10 @@ struct Ctx {
   // cached CUDA graphs of CG batches
   cudaGraphExec_t cg_graph[kGraphSlots] = {};
   int cg_graph_batch[kGraphSlots] = {};
+  // what a cached graph baked in: value and diagonal arrays, storage and SpMV form
+  const void* cg_graph_val[kGraphSlots] = {};
   const void* cg_graph_key[kGraphSlots] = {};
+  int cg_graph_form[kGraphSlots] = {};
   std::vector<cudaEvent_t> ev_pool;
 };
 
