@@ -10,7 +10,10 @@
 // 16 right-hand sides) with one 16-byte load each: every x load of a warp
 // touches 32/tpr lines, each in full, which keeps the L1 wavefronts per byte
 // low; the 9 values of a stored block are loaded once per thread (the lanes of
-// a row share them) and the row sums stay in registers.  The vector kernels
+// a row share them) and the row sums stay in registers.  With 4 to 32
+// right-hand sides the product (k_bspmv_pipe) streams each warp task's values,
+// columns and x lines through a shared-memory ring with cp.async, so that the
+// waits for memory hold no registers.  The vector kernels
 // give every thread the same G right-hand sides of successive dofs.
 // Each right-hand side has its own alpha, beta and stop test; a converged
 // right-hand side is frozen (alpha = beta = 0) while the others continue.
