@@ -353,8 +353,11 @@ typedef struct {
  *      ufc_core/L0_Global/UFC_GlobalContainer_Core.f90) ---- */
 int ufc_ctx_create(int32_t device, ufc_ctx** ctx);
 int ufc_ctx_destroy(ufc_ctx* ctx);
-/* Use a caller-owned cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream); NULL = own stream. */
+/* Use a caller-owned cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream); NULL = own stream.
+ * No counterpart in the reference, which runs on the CPU. */
 int ufc_ctx_set_stream(ufc_ctx* ctx, void* cuda_stream);
+/* Time every SpMV of the following solves with CUDA events (read with
+ * ufc_last_timing); no counterpart in the reference. */
 int ufc_ctx_set_instrument(ufc_ctx* ctx, int32_t on);
 /* ErrorStatusType%message (IF_Err_Def.f90:118-135) of the last failure. */
 int ufc_last_error(const ufc_ctx* ctx, char* buf, int32_t buflen);
@@ -421,6 +424,7 @@ int ufc_mg_level_info(ufc_ctx* ctx, int32_t level, int64_t* n_dof, int64_t* nnz)
 int ufc_mg_export(ufc_ctx* ctx, int32_t level, const ufc_csr_export_arg* arg);
 int ufc_pcg_solve_block(ufc_ctx* ctx, int32_t nrhs, const double* B, double* X, int32_t mem,
                         const ufc_solver_algo* algo, ufc_solver_state* states);
+/* Device-time counters of the last solve (ufc_timing_info); no counterpart in the reference. */
 int ufc_last_timing(const ufc_ctx* ctx, ufc_timing_info* info);
 /* NM_Solver_State%residual_history (NM_Solv_Def.f90:114) of the last solve:
  * ||r_k||_2 of the CG recurrence after each iteration k (host array, at most
@@ -434,10 +438,13 @@ int ufc_nr_increment(ufc_ctx* ctx, ufc_nr_arg* arg);
 int ufc_nr_step(ufc_ctx* ctx, ufc_step_arg* arg);
 int ufc_state_commit(ufc_ctx* ctx);
 int ufc_state_rollback(ufc_ctx* ctx);
-/* Current displacement held by the context ([n_dof]). */
+/* Current displacement held by the context ([n_dof]): the Newton state's u of
+ * RT_NLSolver_NewtonRaph (ufc_core/L5_RT/Solver/RT_Solv_Nonlin.f90:807-830). */
 int ufc_get_displacement(ufc_ctx* ctx, double* u, int32_t mem);
 int ufc_set_displacement(ufc_ctx* ctx, const double* u, int32_t mem);
-/* Committed J2 state: eps_p_eq [n_elems*8], stress [n_elems*8][6], eps_p [n_elems*8][6]; any may be NULL. */
+/* Committed J2 state: eps_p_eq [n_elems*8], stress [n_elems*8][6], eps_p [n_elems*8][6]; any may be NULL
+ * (the solution-dependent variables sdv(1) and sdv(2:7) and the stress of
+ * PH_Mat_Plast_J2_Iso_Core.f90:91-93 and PH_Mat_Reg.f90:232-235). */
 int ufc_get_state(ufc_ctx* ctx, double* eps_p_eq, double* stress, double* eps_p, int32_t mem);
 
 /* ---- adjoint: dJ/dE_e = -sum_k lambda_k,e^T (dK_e/dE_e) u_k,e for nrhs pairs
