@@ -49,6 +49,9 @@ def lib():
         L.orc_spmv.argtypes = [C.c_int64, _i64, _i32, _d, _d, _d]
         L.orc_pcg.argtypes = [C.c_int64, _i64, _i32, _d, _d, _d, C.c_double, C.c_double, C.c_int,
                               C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_pcg_marked.argtypes = [C.c_int64, _i64, _i32, _d, _d, _d, C.c_double, C.c_int, C.c_double, _d,
+                                     C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_double)]
         L.orc_fint.argtypes = [C.c_int32, C.c_int32, _d, _i32, _d, C.c_int32, C.c_int, _d, C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _i32, C.c_int,
                                _d]
@@ -255,6 +258,23 @@ def pcg(K: CSR, b, x0=None, rtol=1e-10, atol=0.0, max_iter=100000):
     st = lib().orc_pcg(K.n, K.row_ptr, K.col, K.val, np.ascontiguousarray(b, dtype=np.float64), x, rtol, atol,
                        max_iter, C.byref(it), C.byref(rf), C.byref(ri))
     return x, {"status": st, "iters": it.value, "res_final": rf.value, "res_init": ri.value}
+
+
+def pcg_marked(K: CSR, b, rtol=1e-13, mark_rtol=1e-10, max_iter=100000):
+    """Jacobi-PCG from x0 = 0 to rtol, recording on the way the iterate, the
+    iteration count and the wall time (setup included) at which the recursive
+    residual first met mark_rtol: one run gives both the tightly converged
+    reference solution and the time of the iter_pcg solve to mark_rtol
+    (ufc_core/L2_NM/Solver/LinSolv/NM_Solv_IterSolver.f90:713-846)."""
+    x = np.zeros(K.n)
+    x_mark = np.zeros(K.n)
+    it, it_mark = C.c_int(0), C.c_int(-1)
+    rf, t_mark = C.c_double(0.0), C.c_double(-1.0)
+    st = lib().orc_pcg_marked(K.n, K.row_ptr, K.col, K.val, np.ascontiguousarray(b, dtype=np.float64), x, rtol,
+                              max_iter, mark_rtol, x_mark, C.byref(it_mark), C.byref(t_mark), C.byref(it),
+                              C.byref(rf))
+    return x, x_mark, {"status": st, "iters": it.value, "res_final": rf.value, "mark_iters": it_mark.value,
+                       "mark_s": t_mark.value}
 
 
 def nr_increment_j2(model: Model, u, state, tgt, tol=1e-8, max_iter=25, lin_rtol=1e-10):

@@ -454,9 +454,18 @@ static double orc_dot(int64_t n, const double* a, const double* b) {
  * diag_inv = 1/K_ii, or 1 when |K_ii| <= 1e-30 (NM_Solv_LinPrec.f90:312-353).
  * x is the initial guess on entry.  max_iter <= 0 means "time exactly
  * |max_iter| iterations" (no convergence exit), used by the CPU baseline.
+ * When mark_rtol > 0, the first iterate whose recursive residual is at most
+ * mark_rtol*||b|| is copied to x_mark, with its iteration count and the wall
+ * time from entry (setup included, the copy excluded): the run an iter_pcg
+ * call with rtol = mark_rtol would have made, taken on the way to rtol.
  * Returns ORC_OK, ORC_NOT_CONVERGED or ORC_ERROR (breakdown). */
-int orc_pcg(int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val, const double* b, double* x,
-            double rtol, double atol, int max_iter, int* iters, double* res_final, double* res_init) {
+static int pcg_impl(int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val, const double* b,
+                    double* x, double rtol, double atol, int max_iter, int* iters, double* res_final,
+                    double* res_init, double mark_rtol, double* x_mark, int* it_mark, double* t_mark) {
+  const double t_start = omp_get_wtime();
+  double mark_tol = -1.0;
+  if (it_mark) *it_mark = -1;
+  if (t_mark) *t_mark = -1.0;
   double* r = (double*)malloc(sizeof(double) * (size_t)n);
   double* z = (double*)malloc(sizeof(double) * (size_t)n);
   double* p = (double*)malloc(sizeof(double) * (size_t)n);
@@ -479,6 +488,7 @@ int orc_pcg(int64_t n, const int64_t* row_ptr, const int32_t* col, const double*
   if (res_init) *res_init = rnorm;
   if (bnorm < 1e-30) bnorm = 1.0;
   double tol = rtol * bnorm > atol ? rtol * bnorm : atol;
+  if (mark_rtol > 0.0 && x_mark) mark_tol = mark_rtol * bnorm;
   int status = ORC_NOT_CONVERGED, k = 0;
   if (rnorm <= tol && !fixed_count) {
     status = ORC_OK;
@@ -506,6 +516,12 @@ int orc_pcg(int64_t n, const int64_t* row_ptr, const int32_t* col, const double*
       rr += r[i] * r[i];
     }
     rnorm = sqrt(rr);
+    if (mark_tol > 0.0 && rnorm <= mark_tol) {
+      if (t_mark) *t_mark = omp_get_wtime() - t_start;
+      if (it_mark) *it_mark = k;
+      memcpy(x_mark, x, sizeof(double) * (size_t)n);
+      mark_tol = -1.0;
+    }
     if (rnorm <= tol && !fixed_count) {
       status = ORC_OK;
       break;
@@ -531,6 +547,19 @@ done:
   if (res_final) *res_final = rnorm;
   free(r); free(z); free(p); free(q); free(dinv);
   return status;
+}
+
+int orc_pcg(int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val, const double* b, double* x,
+            double rtol, double atol, int max_iter, int* iters, double* res_final, double* res_init) {
+  return pcg_impl(n, row_ptr, col, val, b, x, rtol, atol, max_iter, iters, res_final, res_init, 0.0, NULL, NULL,
+                  NULL);
+}
+
+int orc_pcg_marked(int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val, const double* b,
+                   double* x, double rtol, int max_iter, double mark_rtol, double* x_mark, int* it_mark,
+                   double* t_mark, int* iters, double* res_final) {
+  return pcg_impl(n, row_ptr, col, val, b, x, rtol, 0.0, max_iter, iters, res_final, NULL, mark_rtol, x_mark,
+                  it_mark, t_mark);
 }
 
 /* Internal force F_int = sum_e sum_gp w detJ B^T sigma (PH_Elem_C3D8_IntForce,
