@@ -115,8 +115,10 @@ def test_cantilever_40x8x8_solve(pkg, orc, prec):
     # independent FP64 residual with the oracle's matrix
     r = b - info["K"].matvec(u)
     assert np.linalg.norm(r) / np.linalg.norm(b) <= 2e-10
+    # displacement error against the oracle solved to rtol 1e-13: at most 1e-9
+    # relative (the accuracy target of the path; measured about 1e-12)
     err = np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref)
-    assert err <= 1e-8, err
+    assert err <= 1e-9, err
     if prec == "fp64":
         _, info10 = ref.solve_linear(rtol=1e-10)
         assert abs(st.niter - info10["iters"]) <= 3, (st.niter, info10["iters"])
@@ -142,7 +144,7 @@ def test_symmetric_storage_matches_full(pkg, orc, shape):
     for prec in (pkg.PRECISION_FP64, pkg.PRECISION_FP32_REFINE):
         u, st = sym.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=prec))
         assert st.converged and st.rnorm <= 1e-10
-        assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-8
+        assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-9
     # the canonical export is unchanged by the symmetric copies
     _, _, v, _ = sym.csr_export()
     assert np.abs(v - K.val).max() <= 1e-12 * np.abs(K.val).max()
@@ -204,6 +206,35 @@ def test_not_converged_and_errors(pkg):
     assert m2.solve(pkg.lifted_rhs(m2, m2.problem.f))[1].converged
 
 
+@pytest.mark.parametrize("precond", ["jacobi", "multigrid", "block"])
+def test_nan_load_returns_status(pkg, precond):
+    """A load vector holding a NaN (or an Inf) is rejected with
+    IF_STATUS_INVALID before any iteration (RT_Step_Exec.f90:560-600 reports a
+    failed increment by status, never by hanging); the model stays usable."""
+    p = pkg.mesh.lognormal_cantilever(8, 4, 4, seed=3)
+    m = _model(pkg, p, pkg.BUILD_FP64 | pkg.BUILD_FP32_ROUNDED)
+    b = pkg.lifted_rhs(m, p.f)
+    bad = b.copy()
+    bad[np.nonzero(b)[0][0]] = np.nan
+    if precond == "multigrid":
+        m.mg_setup(8, 4, 4)
+        algos = [pkg.SolverAlgo(tolerance=1e-10, precond_type=pkg.SOLV_PREC_MG)]
+    else:
+        algos = [pkg.SolverAlgo(tolerance=1e-10, precision_mode=pm)
+                 for pm in (pkg.PRECISION_FP64, pkg.PRECISION_FP32_REFINE)]
+    for algo in algos:
+        for v in (np.nan, np.inf):
+            bad[np.nonzero(b)[0][0]] = v
+            with pytest.raises(pkg.UfcError) as ei:
+                if precond == "block":
+                    m.solve_block(np.stack([b, bad]), algo)
+                else:
+                    m.solve(bad, algo)
+            assert ei.value.status_code == pkg.STATUS_INVALID and "non-finite" in ei.value.message
+        _, st = m.solve(b, algo)
+        assert st.converged and st.rnorm <= 1e-10
+
+
 @pytest.mark.parametrize("nrhs", [1, 2, 3, 8, 16, 32])
 def test_block_solve_matches_single(pkg, orc, nrhs):
     p = pkg.mesh.density_problem(10, 5, 5, seed=5, n_rhs=max(nrhs, 1))
@@ -217,5 +248,5 @@ def test_block_solve_matches_single(pkg, orc, nrhs):
         r = F[k] - K.matvec(X[k])
         assert np.linalg.norm(r) / np.linalg.norm(F[k]) <= 2e-10
         x1, s1 = m.solve(F[k], algo)
-        assert np.linalg.norm(X[k] - x1) <= 1e-8 * np.linalg.norm(x1)
+        assert np.linalg.norm(X[k] - x1) <= 1e-9 * np.linalg.norm(x1)
         assert abs(states[k].niter - s1.niter) <= 2

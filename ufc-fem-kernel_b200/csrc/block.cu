@@ -647,10 +647,17 @@ static int pcg_block_run(BlockRun& B, int nrhs, const ufc_solver_algo* algo, BSc
     return UFC_STATUS_OK;
   };
   UFC_TRY(residual());
+  for (int k = 0; k < nrhs; ++k) {
+    if (!std::isfinite(hs->bb[k]))
+      return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve_block: non-finite right-hand side " + std::to_string(k));
+    if (!std::isfinite(hs->true_rr[k]))
+      return fail(c, UFC_STATUS_INVALID,
+                  "ufc_pcg_solve_block: non-finite initial residual of right-hand side " + std::to_string(k));
+  }
   for (int k = 0; k < nr; ++k) {
     const double bn = std::sqrt(hs->bb[k]);
     bnorm[k] = bn < 1e-30 ? 1.0 : bn;
-    tol[k] = std::max(algo->tolerance * bnorm[k], algo->abs_tolerance);
+    tol[k] = kStopMargin * std::max(algo->tolerance * bnorm[k], algo->abs_tolerance);
     if (k < nrhs) st[k].initial_residual = std::sqrt(hs->true_rr[k]);
   }
   const int batch = algo->check_every > 0 ? algo->check_every : 32;

@@ -85,6 +85,12 @@ int vec_grid(int64_t n) {
 
 enum SpmvMode { kPlain = 0, kCg = 1 };
 
+// The kernels of a CG iteration do nothing once the run has stopped or asked
+// for an FP64 residual replacement: a batch of iterations launched as one graph
+// then idles from the triggering iteration on, so the replacement happens at
+// that iteration (before its direction update) and not at the end of the batch.
+__device__ __forceinline__ bool halted(const CgScalars* s) { return (s->stop | s->want_update) != 0; }
+
 // y = K x, one thread per block row of a SELL-32 slice (a warp = a slice).
 // TV: stored value type, TX: vector type, TA: accumulator type of the row sums.
 // DIFF: values in difference form (diagonal slot = block row sum S_i), so the
@@ -95,7 +101,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
            const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y, CgScalars* __restrict__ scal,
            double* __restrict__ partials) {
   pdl_enter();
-  if (MODE == kCg && scal->stop) return;
+  if (MODE == kCg && halted(scal)) return;
   const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
   double dot[1] = {0.0};
   if (row < nrows_pad) {
@@ -159,7 +165,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
            const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y, CgScalars* __restrict__ scal,
            double* __restrict__ partials) {
   pdl_enter();
-  if (MODE == kCg && scal->stop) return;
+  if (MODE == kCg && halted(scal)) return;
   constexpr int kWarps = kSpmvBlock / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int part = warp % SPLIT;
@@ -316,7 +322,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
                const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y,
                CgScalars* __restrict__ scal, double* __restrict__ partials) {
   pdl_enter();
-  if (MODE == kCg && scal->stop) return;
+  if (MODE == kCg && halted(scal)) return;
   const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
   double dot[1] = {0.0};
   if (row < nrows_pad) {
@@ -416,7 +422,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
                      const int32_t* __restrict__ lcol, const TV* __restrict__ val, const TX* __restrict__ x,
                      TX* __restrict__ y, CgScalars* __restrict__ scal, double* __restrict__ partials) {
   pdl_enter();
-  if (MODE == kCg && scal->stop) return;
+  if (MODE == kCg && halted(scal)) return;
   constexpr int kWarps = kSpmvBlock / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int part = warp % SPLIT;
@@ -522,7 +528,7 @@ __global__ void __launch_bounds__(kVecBlock)
                 double* __restrict__ x, const T* __restrict__ dinv, CgScalars* __restrict__ scal,
                 double* __restrict__ partials) {
   pdl_enter();
-  if (scal->stop) return;
+  if (halted(scal)) return;
   const double alpha = scal->alpha;
   const T a = (T)alpha;
   T rz = T(0), rr = T(0);
@@ -579,7 +585,7 @@ __global__ void __launch_bounds__(kVecBlock)
     k_cg_pupdate(int64_t n, const T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ p,
                  const CgScalars* __restrict__ scal) {
   pdl_enter();
-  if (scal->stop) return;
+  if (halted(scal)) return;
   const T beta = (T)scal->beta;
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t n4 = n >> 2;
@@ -859,9 +865,12 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
   UFC_CUDA(c, cudaMemcpyAsync(c->scal, &h, sizeof(CgScalars), cudaMemcpyHostToDevice, c->stream));
   UFC_TRY(true_residual(R, true));
   UFC_TRY(read_scalars(c));
+  if (!std::isfinite(c->h_scal->bb)) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: non-finite right-hand side");
+  if (!std::isfinite(c->h_scal->true_rr))
+    return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: non-finite initial residual (initial guess or matrix)");
   const double bnorm_raw = std::sqrt(c->h_scal->bb);
   const double bnorm = bnorm_raw < 1e-30 ? 1.0 : bnorm_raw;
-  const double tol = std::max(algo->tolerance * bnorm, algo->abs_tolerance);
+  const double tol = kStopMargin * std::max(algo->tolerance * bnorm, algo->abs_tolerance);
   st->initial_residual = std::sqrt(c->h_scal->true_rr);
   double true_rr = c->h_scal->true_rr;
   int flag = 0;
@@ -886,7 +895,7 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
     int slot = 0, in_flight = 0, iter_seen = 0;
     int stall = 0, restarts = 0;
     double best_rr = true_rr;
-    constexpr int kMaxStall = 12;      // replacements without a 4x drop of ||b - K x||^2
+    constexpr int kMaxStall = 3;       // replacements without a 4x drop of ||b - K x||^2
     constexpr int kMaxRestarts = 4;    // restarts after a breakdown of the recurrence
     constexpr double kDiverge = 1e4;   // ||b - K x|| grew 100x above the best seen
     const bool keep_best = c->xb64 != nullptr;
@@ -976,7 +985,9 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
         }
         break;
       }
-      int mode = cur.stop == 1 ? 1 : 0;
+      // the iteration kernels halt right after the update that stopped the run or
+      // asked for the replacement, before its direction update (mode 1)
+      int mode = 1;
       if (cur.stop == 3) {
         // breakdown of the recurrence: restart CG from the FP64 residual
         if (++restarts > kMaxRestarts) {
