@@ -413,8 +413,8 @@ int ufc_spmv(ufc_ctx* ctx, int32_t precision, const void* x, void* y, int32_t me
  * UFC_STATUS_NOT_CONVERGED when max_iter is reached. */
 int ufc_pcg_solve(ufc_ctx* ctx, const double* b, double* x, int32_t mem, const ufc_solver_algo* algo,
                   ufc_solver_state* state);
-/* nrhs independent Jacobi-PCG solves sharing every SpMV (one matrix read per
- * iteration for all right-hand sides).  B and X are [nrhs][n_dof]; states[nrhs]. */
+/* Builds the geometric multigrid hierarchy described at ufc_mg_arg (in the place
+ * of NM_AMG_Setup, NM_Solv_LinPrecAMG.f90:120-675). */
 int ufc_mg_setup(ufc_ctx* ctx, ufc_mg_arg* arg);
 /* z = M r: one V-cycle of the multigrid preconditioner ([n_dof] vectors). */
 int ufc_mg_apply(ufc_ctx* ctx, const double* r, double* z, int32_t mem);
@@ -422,6 +422,8 @@ int ufc_mg_apply(ufc_ctx* ctx, const double* r, double* z, int32_t mem);
  * matrix), as ufc_csr_export; ufc_mg_level_info gives its DOF and non-zeros. */
 int ufc_mg_level_info(ufc_ctx* ctx, int32_t level, int64_t* n_dof, int64_t* nnz);
 int ufc_mg_export(ufc_ctx* ctx, int32_t level, const ufc_csr_export_arg* arg);
+/* nrhs independent Jacobi-PCG solves sharing every SpMV (one matrix read per
+ * iteration for all right-hand sides).  B and X are [nrhs][n_dof]; states[nrhs]. */
 int ufc_pcg_solve_block(ufc_ctx* ctx, int32_t nrhs, const double* B, double* X, int32_t mem,
                         const ufc_solver_algo* algo, ufc_solver_state* states);
 /* Device-time counters of the last solve (ufc_timing_info); no counterpart in the reference. */
@@ -458,15 +460,18 @@ int ufc_adjoint_sensitivity(ufc_ctx* ctx, int32_t nrhs, const double* U, const d
  * y = A x and *xy = x.y for a caller-owned FP64 CSR matrix (0-based row_ptr,
  * col_ind, values, e.g. from ufc_csr_export with mem = UFC_MEM_DEVICE), all
  * pointers in device memory, enqueued on cuda_stream (NULL: legacy stream).
- * It is for callers that cannot allocate device memory -- a solver loop being
- * captured into a CUDA graph, or a host code that owns all device memory in its
- * own pool: it calls no cudaMalloc/cudaFree and needs no context.  The
- * dot-product scratch is a static device array: at most UFC_NOALLOC_MAX_ROWS
- * rows (larger calls return UFC_STATUS_INVALID); each GPU that loads the library
- * keeps the array (about 512 KiB) until exit; the first call on a device looks
- * up its address and should come before any stream capture; calls that overlap
- * on the GPU share the array and race, so the caller serialises them.  The
- * message of a failure is written to errbuf (may be NULL). */
+ * It is for callers that cannot allocate device memory -- a host code whose
+ * device memory all comes from its own fixed pool, or one that may not enter
+ * the CUDA allocator on its hot path: it calls no cudaMalloc/cudaFree and needs
+ * no context.  The dot-product scratch is a static device array: at most
+ * UFC_NOALLOC_MAX_ROWS rows (larger calls return UFC_STATUS_INVALID); each GPU
+ * that loads the library keeps the array (about 512 KiB) until exit; the first
+ * call on a device looks up its address and should come before any stream
+ * capture, and that address is not looked up again (do not use the entry point
+ * on a device after a cudaDeviceReset of it); cuda_stream must belong to the
+ * current device (else UFC_STATUS_INVALID); calls that overlap on the GPU share
+ * the array and race, so the caller serialises them.  The message of a failure
+ * is written to errbuf (may be NULL). */
 #define UFC_NOALLOC_MAX_ROWS 16777216
 int ufc_csr_spmv_dot_noalloc(int64_t n_rows, const int64_t* row_ptr, const int32_t* col_ind,
                              const double* values, const double* x, double* y, double* xy, void* cuda_stream,

@@ -1,0 +1,73 @@
+"""The reference's call surface (ufc_api) over the GPU path: NM_Solver_PCG,
+PH_Mat_UpdateStress, RT_Asm_GlobalStiffness / RT_Asm_ComputeResidual and
+RT_NLSolver_NewtonRaph return statuses as the Fortran routines do and agree
+with the oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_nm_solver_pcg_matches_oracle_and_reports_status(pkg, orc):
+    api = pkg.ufc_api
+    p = pkg.mesh.lognormal_cantilever(16, 8, 8, seed=2)
+    ctx = api.NM_Solver_Ctx(pkg.FemModel.from_problem(p))
+    assert api.RT_Asm_GlobalStiffness(ctx).ok
+    b = pkg.lifted_rhs(ctx.model, p.f)
+    desc = api.NM_Solver_Desc(n=p.n_dof, is_symmetric=True, is_spd=True)
+    algo = api.NM_Solver_Algo(method=api.NM_SOLV_METHOD_CG, precond_type=api.NM_SOLV_PREC_JACOBI)
+    algo.SetTolerance(1e-10)
+    state = api.NM_Solver_State(b=b)
+    status = api.NM_Solver_PCG(desc, state, algo, ctx)
+    assert status.status_code == api.IF_STATUS_OK and state.converged and state.rnorm <= 1e-10
+    u_ref, _ = orc.Model(p).solve_linear(rtol=1e-13)
+    assert np.linalg.norm(state.x - u_ref) / np.linalg.norm(u_ref) <= 1e-9
+    # residual history: one entry per iteration, ending at the recursive residual
+    assert state.residual_history.size == state.niter and np.all(np.isfinite(state.residual_history))
+    # R = F_ext - F_int(u) is at the solver tolerance on the free DOFs
+    R, st = api.RT_Asm_ComputeResidual(ctx, state.x, b)
+    assert st.ok and np.linalg.norm(R) <= 2e-10 * np.linalg.norm(b)
+    # max_iter reached: IF_STATUS_NOT_CONVERGED and the reference's message
+    algo.SetMaxIter(3)
+    state = api.NM_Solver_State(b=b)
+    status = api.NM_Solver_PCG(desc, state, algo, ctx)
+    assert status.status_code == api.IF_STATUS_NOT_CONVERGED and "did not converge" in status.message
+    assert state.niter == 3 and not state.converged
+    # wrong dimension: IF_STATUS_INVALID, nothing run
+    status = api.NM_Solver_PCG(api.NM_Solver_Desc(n=p.n_dof + 3), api.NM_Solver_State(b=b), algo, ctx)
+    assert status.status_code == api.IF_STATUS_INVALID
+    ctx.model.close()
+
+
+def test_material_update_known_answer(pkg):
+    api = pkg.ufc_api
+    ctx = api.NM_Solver_Ctx(pkg.FemModel())
+    # ufc_core/Testing/test_defn_invoke_umat.f90:43: sigma11 = 282.69230769230769
+    arg = api.PH_Mat_Update_Arg(101, np.array([210000.0, 0.3]), np.zeros(6), np.array([1e-3, 0, 0, 0, 0, 0]))
+    assert api.PH_Mat_UpdateStress(ctx, arg).ok
+    assert abs(arg.stress_new[0, 0] - 282.69230769230769) <= 1e-12 * 282.7
+    # an unknown material id is a status, not an exception
+    bad = api.PH_Mat_Update_Arg(999, np.array([210000.0, 0.3]), np.zeros(6), np.zeros(6))
+    assert api.PH_Mat_UpdateStress(ctx, bad).status_code != api.IF_STATUS_OK
+
+
+def test_newton_increment_and_step_driver(pkg, orc):
+    api = pkg.ufc_api
+    p = pkg.mesh.j2_bar(4, 2, 2)
+    targets = [pkg.mesh.j2_bar_target(p, s, n_steps=4, strain=0.006) for s in range(1, 5)]
+    hist, _, _ = orc.nr_j2(orc.Model(p), targets)
+    ctx = api.NM_Solver_Ctx(pkg.FemModel.from_problem(p))
+    solver = api.MD_NonlinSolv(max_iterations=25, tolerance_force=1e-8, linear=pkg.SolverAlgo(tolerance=1e-12))
+    for s, tgt in enumerate(targets):
+        state = api.MD_SolverState()
+        result, status = api.RT_NLSolver_NewtonRaph(solver, state, ctx, tgt)
+        assert result and status.ok and state.converged and state.iteration <= 8
+        ctx.model.commit()
+        u = ctx.model.displacement()
+        np.testing.assert_allclose(u, hist[s], rtol=0, atol=1e-9 * np.abs(hist[s]).max())
+    # a step that cannot converge reports IF_STATUS_NOT_CONVERGED through the step driver
+    stuck = api.MD_NonlinSolv(max_iterations=1, tolerance_force=1e-14, linear=pkg.SolverAlgo(tolerance=1e-12))
+    res, status = api.RT_StepDriver_Execute(ctx, stuck, targets[-1] * 2.0, dt_initial=1.0, dt_min=0.2,
+                                            max_cutbacks=1)
+    assert status.status_code == api.IF_STATUS_NOT_CONVERGED and res is not None and not res.completed
+    ctx.model.close()

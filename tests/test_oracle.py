@@ -75,8 +75,6 @@ def test_j2_consistent_tangent_fd(orc):
 
 
 def test_j2_tensor_form_agrees(orc):
-    for st in REG["j2_mixed_history"]["steps"]:
-        pass
     props = REG["j2_mixed_history"]["props"]
     sig, ep, prev = np.zeros(6), 0.0, np.zeros(6)
     epl = np.zeros(6)

@@ -11,7 +11,7 @@ include/ufc_gpu.h); this package is its Python host side:
   hand-written adjoint;
 * :mod:`.mesh`     -- seeded structured meshes, Dirichlet sets and loads.
 """
-from . import _abi, mesh  # noqa: F401
+from . import _abi, mesh, ufc_api  # noqa: F401
 from ._abi import LibraryMissing, check_abi, load  # noqa: F401
 from .fem import FemModel, NrResult, SolverAlgo, SolverState, StepResult, UfcError, lifted_rhs  # noqa: F401
 

@@ -26,6 +26,9 @@ import torch
 from . import _abi as A
 from .fem import FemModel, SolverAlgo
 
+# largest block of right-hand sides ufc_pcg_solve_block takes in one call
+MAX_BLOCK_RHS = 32
+
 
 class ElasticModel:
     """A FemModel whose per-element moduli can change between solves."""
@@ -53,16 +56,23 @@ class ElasticModel:
         return True
 
     def solve(self, B: torch.Tensor, algo: SolverAlgo):
-        """Solve K X = P B for each row of B ([nrhs, n] or [n])."""
+        """Solve K X = P B for each row of B ([nrhs, n] or [n]).  With the
+        Jacobi preconditioner, 2 to 32 right-hand sides are solved together by
+        the block PCG (ufc_pcg_solve_block: one pass over K per iteration for
+        all of them, each with its own recurrence and stop test); with the
+        multigrid preconditioner, or more than 32, one after another."""
         single = B.dim() == 1
         B2 = (B.reshape(-1, B.shape[-1]) * self.free).contiguous()
-        if B2.shape[0] == 1:
+        nrhs = B2.shape[0]
+        if nrhs == 1:
             X, st = self.fem.solve(B2[0], algo)
             X, states = X.reshape(1, -1), [st]
+        elif algo.precond_type == A.SOLV_PREC_JACOBI and nrhs <= MAX_BLOCK_RHS:
+            X, states = self.fem.solve_block(B2, algo)
         else:
             X = torch.empty_like(B2)
             states = []
-            for k in range(B2.shape[0]):
+            for k in range(nrhs):
                 _, st = self.fem.solve(B2[k], algo, x=X[k])
                 states.append(st)
         self.last_states = states
@@ -99,3 +109,48 @@ def compliance(E, F, model, algo=None):
     """J = sum_k F_k . U_k with U = K(E)^-1 P F."""
     U = UfcLinearElastic.apply(E, F, model, algo)
     return (F * U).sum(), U
+
+
+def density_objectives(rho, F, model, algo=None, tip_dof=None, E0=210e3, power=3.0):
+    """The two objectives of a density problem, summed over its load cases
+    (rows of F): compliance J1 = sum_k F_k . U_k and, when tip_dof is given,
+    the displacement J2 = sum_k U_k[tip_dof], with U = K(E0 rho^power)^-1 P F
+    solved by UfcLinearElastic (one block solve for up to 32 Jacobi cases).
+    Returns (J1, J2 or None, U)."""
+    U = UfcLinearElastic.apply(E0 * rho ** power, F, model, algo)
+    J1 = (F * U).sum()
+    J2 = U[..., tip_dof].sum() if tip_dof is not None else None
+    return J1, J2, U
+
+
+def central_differences(model, rho, F, U0, elems, algo, tip_dof=None, h=1e-6, E0=210e3, power=3.0):
+    """Central finite differences of the density_objectives with respect to
+    rho at the elements `elems` (a gradient check of the adjoint).  Each
+    perturbed displacement is solved as a correction K' D = P (F - K' U0) from
+    the unperturbed U0 ([nrhs, n]), and the two perturbed objectives are
+    differenced through their corrections alone, so the difference is not
+    swamped by the solver tolerance.  The moduli of rho are restored on exit.
+    Returns (dJ1/drho, dJ2/drho) at the elements (the second None without
+    tip_dof), as host lists."""
+    F2 = F.reshape(-1, F.shape[-1])
+    U2 = U0.reshape(-1, U0.shape[-1]).detach()
+    base = rho.detach()
+    d1, d2 = [], []
+    try:
+        for e in elems:
+            vals = []
+            for sgn in (1.0, -1.0):
+                r = base.clone()
+                r[int(e)] += sgn * h
+                model.set_moduli(E0 * r ** power)
+                R = torch.empty_like(U2)
+                for k in range(U2.shape[0]):
+                    _, R[k], _, _ = model.fem.internal_force(U2[k].contiguous(), f_ext=F2[k].contiguous(),
+                                                             update_state=False)
+                D, _ = model.solve(R, algo)
+                vals.append(((F2 * D).sum().item(), D[:, tip_dof].sum().item() if tip_dof is not None else 0.0))
+            d1.append((vals[0][0] - vals[1][0]) / (2 * h))
+            d2.append((vals[0][1] - vals[1][1]) / (2 * h))
+    finally:
+        model.set_moduli(E0 * base ** power)
+    return d1, (d2 if tip_dof is not None else None)

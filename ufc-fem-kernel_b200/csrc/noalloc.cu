@@ -1,14 +1,15 @@
 // ufc_csr_spmv_dot_noalloc: y = A x and x.y on a caller-owned CSR matrix,
 // for callers that cannot allocate device memory.
 //
-// Who needs it: host codes that own every device buffer themselves and forbid
-// allocation on their hot path -- a solver loop that is being recorded into a
-// CUDA graph (cudaMalloc is not allowed while a stream is captured), or a host
-// program whose device memory comes from its own fixed pool and whose
-// allocator must not be bypassed.  They pass the matrix and vectors; the only
-// scratch the kernel needs, the per-block partial sums of the dot product and
-// the counter that elects the block finishing the reduction, lives in a
-// file-scope static device array instead of an allocation.
+// Who needs it: host codes that own every device buffer themselves and may not
+// allocate on their hot path -- a Fortran or C solver whose device memory all
+// comes from its own fixed pool (its allocator must not be bypassed, and its
+// budget is fixed when the run starts), or code running where a call to
+// cudaMalloc would synchronise the device and stall work the caller keeps in
+// flight.  They pass the matrix and vectors; the only scratch the kernel needs,
+// the per-block partial sums of the dot product and the counter that elects
+// the block finishing the reduction, lives in a file-scope static device array
+// instead of an allocation.
 //
 // Limits and behaviour:
 //  * at most UFC_NOALLOC_MAX_ROWS rows (one thread per row, 256 rows per block,
@@ -17,10 +18,16 @@
 //  * every GPU that loads this library holds the array (about 512 KiB) until the
 //    process exits;
 //  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress; make that first call before any stream capture;
-//  * all calls share the array: calls that overlap on the GPU (on different
-//    streams, or from several threads) race on it and must be serialised by
-//    the caller.
+//    cudaGetSymbolAddress (the host-side name of the array is not a device
+//    address) and keeps it for that device; make that first call before any
+//    stream capture.  A cudaDeviceReset of the device invalidates the kept
+//    address, so the entry point must not be used on a device after resetting
+//    it in the same process;
+//  * the stream must belong to the current device (checked: UFC_STATUS_INVALID
+//    otherwise);
+//  * all calls share the array, and each call clears the counter it needs at
+//    zero: calls that overlap on the GPU (on different streams, or from several
+//    threads) race on the array and must be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -101,6 +108,13 @@ extern "C" int ufc_csr_spmv_dot_noalloc(int64_t n_rows, const int64_t* row_ptr, 
     s = g_scratch_ptr[dev];
   }
   cudaStream_t st = (cudaStream_t)cuda_stream;
+  int stream_dev = dev;
+  if (cudaStreamGetDevice(st, &stream_dev) != cudaSuccess)
+    return set_error(errbuf, errlen, "ufc_csr_spmv_dot_noalloc: invalid stream", UFC_STATUS_INVALID);
+  if (stream_dev != dev)
+    return set_error(errbuf, errlen,
+                     "ufc_csr_spmv_dot_noalloc: the stream belongs to another device than the current one",
+                     UFC_STATUS_INVALID);
   // the election counter must start at zero whatever the last call left there
   if (cudaMemsetAsync(&s->ticket, 0, sizeof(uint32_t), st) != cudaSuccess)
     return set_error(errbuf, errlen, "ufc_csr_spmv_dot_noalloc: cudaMemsetAsync failed", UFC_STATUS_ERROR);
