@@ -219,6 +219,8 @@ def test_nan_load_returns_status(pkg, precond):
     if precond == "multigrid":
         m.mg_setup(8, 4, 4)
         algos = [pkg.SolverAlgo(tolerance=1e-10, precond_type=pkg.SOLV_PREC_MG)]
+    elif precond == "block":  # the block PCG is FP64 only
+        algos = [pkg.SolverAlgo(tolerance=1e-10)]
     else:
         algos = [pkg.SolverAlgo(tolerance=1e-10, precision_mode=pm)
                  for pm in (pkg.PRECISION_FP64, pkg.PRECISION_FP32_REFINE)]
