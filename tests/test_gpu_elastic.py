@@ -252,3 +252,16 @@ def test_block_solve_matches_single(pkg, orc, nrhs):
         x1, s1 = m.solve(F[k], algo)
         assert np.linalg.norm(X[k] - x1) <= 1e-9 * np.linalg.norm(x1)
         assert abs(states[k].niter - s1.niter) <= 2
+
+
+def test_elimination_matches_reference_penalty(pkg, orc):
+    """The GPU's eliminated solve against the reference's penalty treatment of
+    the same Dirichlet set (1e20 max|K_ii| on the diagonal, solved directly on
+    the CPU): within 1e-9 relative, the accuracy target of the path."""
+    from test_oracle import _penalty_solution
+
+    p = pkg.mesh.lognormal_cantilever(8, 4, 4, seed=3)
+    m = _model(pkg, p, pkg.BUILD_FP64)
+    u, st = m.solve(pkg.lifted_rhs(m, p.f), pkg.SolverAlgo(tolerance=1e-12))
+    u_pen = _penalty_solution(p, orc.Model(p).assemble(eliminate=False))
+    assert st.converged and np.linalg.norm(u - u_pen) / np.linalg.norm(u_pen) <= 1e-9
