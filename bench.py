@@ -662,7 +662,7 @@ def run_ours(args):
     e_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     barrier(dev)
     e_ev[0].record(stream)
-    e_steps = max(1, min(args.steps, 3))
+    e_steps = args.steps
     for _ in range(e_steps):
         _, est = m.solve(b_pin, mixed, x=x_pin)
     e_ev[1].record(stream)
@@ -733,9 +733,16 @@ def run_ours(args):
         del sols, vms
 
     mean = lambda xs: sum(xs) / len(xs)  # noqa: E731
+    csr64_bytes = 12 * info["nnz"] + 4 * (info["n_dof"] + 1) + 16 * info["n_dof"] + 88 * info["n_dof"]
+    fp64_csr_s = csr64_bytes / (peak * 1e9) * fst.niter
     line = {
         "metric": METRIC, "value": t_mixed, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": t_mixed * 1e3,
+        "speedup_vs_fp64": t_fp64 / t_mixed,
+        "fp64_path": {"value": t_fp64, "unit": UNIT, "iters": fst.niter, "rnorm": fst.rnorm,
+                      "spmv_achieved_gbs": achieved64,
+                      "dof_iterations_per_s": world * info["n_dof"] * fst.niter / t_fp64},
+        "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (matrix, CG vectors, SpMV rows) + f64 (solution, residual replacement)",
         "data": "synthetic (seeded numpy mesh and moduli)",
         "config": {"workload": workload(args.mesh), "mesh": args.mesh, "n_dof": info["n_dof"], "nnz": info["nnz"],
@@ -750,10 +757,11 @@ def run_ours(args):
         "iters": mean([s.niter for s in states]), "refinements": mean([s.n_refine for s in states]),
         "rnorm": max(s.rnorm for s in states),
         "dof_iterations_per_s": world * info["n_dof"] * mean([s.niter for s in states]) / t_mixed,
-        "fp64_path": {"value": t_fp64, "unit": UNIT, "iters": fst.niter, "rnorm": fst.rnorm,
-                      "spmv_achieved_gbs": achieved64,
-                      "dof_iterations_per_s": world * info["n_dof"] * fst.niter / t_fp64},
-        "speedup_vs_fp64": t_fp64 / t_mixed,
+        "fp64_scalar_csr_equivalent": {
+            "value": fp64_csr_s, "unit": UNIT, "speedup": fp64_csr_s / t_mixed,
+            "model": "the reference's FP64 scalar CSR form (RT_CSRMatrix_matvec: 12 nnz + 4 (n+1) + 16 n bytes per "
+                     "SpMV) plus FP64 vector updates (88 B/DOF) at the measured copy peak, times this run's FP64 "
+                     "iteration count: a floor for that storage on this GPU, a secondary figure, not the headline"},
         "accuracy_vs_fp64_gpu": {"u_rel_l2": du, "von_mises_rel_max": dvm},
         "assembly": {"pattern_ms": pattern_ms, "fp64_plus_rounded_fp32_ms": asm_ms, "fp32_element_ms": asm32_ms,
                      "with_storage_ms": build_ms,
