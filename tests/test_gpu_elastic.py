@@ -145,6 +145,10 @@ def test_symmetric_storage_matches_full(pkg, orc, shape):
         u, st = sym.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=prec))
         assert st.converged and st.rnorm <= 1e-10
         assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-9
+        # the CG product on this storage adds its transposed halves with integer
+        # atomics: the solve is still bitwise reproducible
+        u2, st2 = sym.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=prec))
+        assert np.array_equal(u, u2) and st2.niter == st.niter
     # the canonical export is unchanged by the symmetric copies
     _, _, v, _ = sym.csr_export()
     assert np.abs(v - K.val).max() <= 1e-12 * np.abs(K.val).max()
