@@ -289,6 +289,19 @@ def linear_static(ufc, local, p, cpu=False):
         if cpu:
             sols[key] = x.cpu().numpy()
             vms[key] = m.stress(x, want_sigma=False)[1].cpu().numpy()
+    if res["fp32_refine"]["fp64_continuation_iters"] == res["fp32_refine"]["iters"]:
+        # the matrix fits in L2, so the refined request ran FP64 iterations; the
+        # FP32 iterations forced on the same problem, for comparison
+        a = ufc.SolverAlgo(tolerance=1e-10, precision_mode=ufc.PRECISION_FP32_REFINE,
+                           refine_policy=ufc.REFINE_FORCE_FP32)
+        x.zero_()
+        m.solve(b, a, x=x, raise_on_not_converged=False)
+        x.zero_()
+        _, st = m.solve(b, a, x=x, raise_on_not_converged=False)
+        res["fp32_forced"] = {"s": st.solve_time / 1e3, "iters": st.niter, "rnorm": st.rnorm,
+                              "converged": st.converged, "fp64_continuation_iters": st.fp64_iters,
+                              "note": "FP32 iterations forced (UFC_REFINE_FORCE_FP32); fp32_refine ran FP64 "
+                                      "iterations because the FP64 matrix is read from L2"}
     # FP64 PCG with the geometric multigrid V-cycle in FP32 (set-up outside the timed solve)
     levels, coarse, setup_ms = m.mg_setup(*p.shape, precision=ufc.PRECISION_FP32_REFINE)
     a = ufc.SolverAlgo(tolerance=1e-10, precond_type=ufc.SOLV_PREC_MG)

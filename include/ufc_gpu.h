@@ -92,9 +92,15 @@ extern "C" {
  * use them when present.  Implies UFC_BUILD_FP64. */
 #define UFC_BUILD_SYMMETRIC 16
 
-/* FP32_REFINE policy at each FP64 residual replacement. */
+/* FP32_REFINE policy at each FP64 residual replacement.  With the first two,
+ * a matrix whose FP64 product reads less than half the L2 cache is solved in
+ * FP64 (the FP32 storage saves no time there: both products run from L2 and
+ * are bound by latency, and the FP32 recursion needs more iterations); the
+ * state then reports every iteration in fp64_iters.  UFC_REFINE_FORCE_FP32
+ * keeps the FP32 iterations whatever the size (direction kept). */
 #define UFC_REFINE_KEEP_DIRECTION 0 /* keep the search direction (reliable update) */
 #define UFC_REFINE_RESTART 1        /* restart CG from the new residual (defect correction) */
+#define UFC_REFINE_FORCE_FP32 2     /* keep the direction, FP32 iterations on any size */
 
 typedef struct ufc_ctx ufc_ctx;
 
@@ -208,7 +214,7 @@ typedef struct {
                              one whenever it fell by this factor (0: default 0.1) */
   int32_t check_every;    /* [IN] iterations per launch batch between host checks (0: default) */
   int32_t use_x0;         /* [IN] 1: x holds the initial guess; 0: x0 = 0 */
-  int32_t refine_policy;  /* [IN] UFC_REFINE_KEEP_DIRECTION or UFC_REFINE_RESTART */
+  int32_t refine_policy;  /* [IN] UFC_REFINE_KEEP_DIRECTION, UFC_REFINE_RESTART or UFC_REFINE_FORCE_FP32 */
   int32_t accumulate;     /* [IN] FP32_REFINE: UFC_ACCUMULATE_STORAGE or UFC_ACCUMULATE_FP64 */
 } ufc_solver_algo;
 

@@ -25,6 +25,7 @@ MODULE ufc_gpu_brg
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_SOLV_PREC_NONE = 0, UFC_PRECISION_FP32_MATRIX = 2
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_ACCUMULATE_STORAGE = 0, UFC_ACCUMULATE_FP64 = 1
   INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_REFINE_KEEP_DIRECTION = 0, UFC_REFINE_RESTART = 1
+  INTEGER(C_INT32_T), PARAMETER, PUBLIC :: UFC_REFINE_FORCE_FP32 = 2
   ! IF_Err_Brg status codes (ufc_core/L1_IF/Error/IF_Err_Brg.f90:95-110)
   INTEGER(C_INT), PARAMETER, PUBLIC :: UFC_STATUS_OK = 0, UFC_STATUS_INVALID = 1, UFC_STATUS_ERROR = 2
   INTEGER(C_INT), PARAMETER, PUBLIC :: UFC_STATUS_CONVERGED = 3, UFC_STATUS_NOT_CONVERGED = 4

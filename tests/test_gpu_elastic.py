@@ -97,7 +97,7 @@ def test_spmv_and_internal_force(pkg, orc):
     assert np.all(r[~free] == 0.0)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fp32_refine"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32_refine", "fp32_forced"])
 def test_cantilever_40x8x8_solve(pkg, orc, prec):
     p = pkg.mesh.config1()
     m = pkg.FemModel.from_problem(p)
@@ -105,13 +105,19 @@ def test_cantilever_40x8x8_solve(pkg, orc, prec):
     ref = orc.Model(p)
     u_ref, info = ref.solve_linear(rtol=1e-13)
     mode = pkg.PRECISION_FP64 if prec == "fp64" else pkg.PRECISION_FP32_REFINE
+    policy = pkg.REFINE_FORCE_FP32 if prec == "fp32_forced" else pkg.REFINE_KEEP_DIRECTION
     b = pkg.lifted_rhs(m, p.f)
-    u, st = m.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=mode))
+    u, st = m.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=mode, refine_policy=policy))
     assert st.converged and st.rnorm <= 1e-10
     if prec == "fp32_refine":
-        # this slender cantilever is too ill-conditioned for an FP32 matrix: the
-        # refined FP32 run stalls and the solve finishes in FP64 on the GPU
-        assert st.fp64_iters > 0
+        # 10k DOF: the FP64 matrix (8 MB) is read from L2, where FP32 storage
+        # saves nothing, so the refined request runs FP64 iterations
+        assert st.fp64_iters == st.niter
+    if prec == "fp32_forced":
+        # forced FP32 iterations on this slender, ill-conditioned cantilever: the
+        # refined run converges with residual replacement, or hands its best
+        # iterate on to FP64 when it stalls; either way to the same tolerance
+        assert st.niter > 0
     # independent FP64 residual with the oracle's matrix
     r = b - info["K"].matvec(u)
     assert np.linalg.norm(r) / np.linalg.norm(b) <= 2e-10
@@ -142,12 +148,14 @@ def test_symmetric_storage_matches_full(pkg, orc, shape):
     b = pkg.lifted_rhs(sym, p.f)
     u_ref, _ = orc.Model(p).solve_linear(rtol=1e-13)
     for prec in (pkg.PRECISION_FP64, pkg.PRECISION_FP32_REFINE):
-        u, st = sym.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=prec))
+        # FP32 iterations forced on this small mesh, to exercise the FP32 kernels
+        algo = pkg.SolverAlgo(tolerance=1e-10, precision_mode=prec, refine_policy=pkg.REFINE_FORCE_FP32)
+        u, st = sym.solve(b, algo)
         assert st.converged and st.rnorm <= 1e-10
         assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-9
         # the CG product on this storage adds its transposed halves with integer
         # atomics: the solve is still bitwise reproducible
-        u2, st2 = sym.solve(b, pkg.SolverAlgo(tolerance=1e-10, precision_mode=prec))
+        u2, st2 = sym.solve(b, algo)
         assert np.array_equal(u, u2) and st2.niter == st.niter
     # the canonical export is unchanged by the symmetric copies
     _, _, v, _ = sym.csr_export()

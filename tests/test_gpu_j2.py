@@ -61,7 +61,8 @@ def test_nr_increments_fp32_refined_inner_solves(pkg, orc):
     targets = [pkg.mesh.j2_bar_target(p, s, n_steps=steps, strain=strain) for s in range(1, steps + 1)]
     hist, state, _ = orc.nr_j2(orc.Model(p), targets)
     m = _bar_model(pkg, p)
-    lin = pkg.SolverAlgo(tolerance=1e-12, precision_mode=pkg.PRECISION_FP32_REFINE)
+    lin = pkg.SolverAlgo(tolerance=1e-12, precision_mode=pkg.PRECISION_FP32_REFINE,
+                         refine_policy=pkg.REFINE_FORCE_FP32)
     for s, tgt in enumerate(targets):
         res = m.nr_increment(tgt, tolerance_force=1e-8, lin=lin)
         assert res.converged and res.iterations <= 8

@@ -27,6 +27,7 @@ BUILD_FP32_DIFF = _abi.BUILD_FP32_DIFF
 BUILD_SYMMETRIC = _abi.BUILD_SYMMETRIC
 REFINE_KEEP_DIRECTION = _abi.REFINE_KEEP_DIRECTION
 REFINE_RESTART = _abi.REFINE_RESTART
+REFINE_FORCE_FP32 = _abi.REFINE_FORCE_FP32
 MAT_ELASTIC_ISO = _abi.MAT_ELASTIC_ISO
 MAT_J2_ISO = _abi.MAT_J2_ISO
 SOLV_PREC_JACOBI = _abi.SOLV_PREC_JACOBI

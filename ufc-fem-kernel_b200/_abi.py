@@ -49,6 +49,7 @@ BUILD_FP32_DIFF = 8
 BUILD_SYMMETRIC = 16
 REFINE_KEEP_DIRECTION = 0
 REFINE_RESTART = 1
+REFINE_FORCE_FP32 = 2
 
 _p = C.c_void_p
 _i32 = C.c_int32

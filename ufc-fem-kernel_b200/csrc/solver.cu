@@ -1586,6 +1586,14 @@ int spmv(Ctx* c, int precision, const void* x, void* y) {
   return UFC_STATUS_OK;
 }
 
+// True when one FP64 product of the stored matrix reads less than half the L2.
+bool fp64_fits_l2(const Ctx* c) {
+  int dev = 0, l2 = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess || l2 <= 0) return false;
+  return spmv_bytes(c, UFC_PRECISION_FP64) < (int64_t)l2 / 2;
+}
+
 int pcg_solve(Ctx* c, const double* b, double* x, const ufc_solver_algo* algo, ufc_solver_state* st) {
   if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: pattern not built");
   if (algo->method != UFC_SOLV_METHOD_CG) return fail(c, UFC_STATUS_UNSUPPORTED, "ufc_pcg_solve: method must be CG");
@@ -1618,6 +1626,19 @@ int pcg_solve(Ctx* c, const double* b, double* x, const ufc_solver_algo* algo, u
     s = pcg_mg(c, algo, st);
     if (s != UFC_STATUS_OK && s != UFC_STATUS_NOT_CONVERGED) return s;
     st->fp64_iters = 0;
+    UFC_CUDA(c, cudaMemcpyAsync(x, c->x64, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream));
+    if (s == UFC_STATUS_NOT_CONVERGED) fail(c, UFC_STATUS_NOT_CONVERGED, "[NM_Solver_PCG]: did not converge");
+    return s;
+  }
+  if (prec == UFC_PRECISION_FP32_REFINE && algo->refine_policy != UFC_REFINE_FORCE_FP32 && c->has_val64 &&
+      fp64_fits_l2(c)) {
+    // a matrix this small is read from L2 in either precision: FP64 iterations
+    ufc_solver_algo a64 = *algo;
+    a64.precision_mode = UFC_PRECISION_FP64;
+    UFC_TRY(ensure_vectors(c, UFC_PRECISION_FP64));
+    s = pcg_run<double, double, double>(c, &a64, st);
+    if (s != UFC_STATUS_OK && s != UFC_STATUS_NOT_CONVERGED) return s;
+    st->fp64_iters = st->niter;
     UFC_CUDA(c, cudaMemcpyAsync(x, c->x64, sizeof(double) * c->n, cudaMemcpyDeviceToDevice, c->stream));
     if (s == UFC_STATUS_NOT_CONVERGED) fail(c, UFC_STATUS_NOT_CONVERGED, "[NM_Solver_PCG]: did not converge");
     return s;
