@@ -153,8 +153,7 @@ def test_symmetric_storage_matches_full(pkg, orc, shape):
         u, st = sym.solve(b, algo)
         assert st.converged and st.rnorm <= 1e-10
         assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-9
-        # the CG product on this storage adds its transposed halves with integer
-        # atomics: the solve is still bitwise reproducible
+        # the solve is bitwise reproducible (no float atomics anywhere)
         u2, st2 = sym.solve(b, algo)
         assert np.array_equal(u, u2) and st2.niter == st.niter
     # the canonical export is unchanged by the symmetric copies

@@ -19,7 +19,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cstring>
 #include <vector>
 
 #include "c3d8_device.cuh"
@@ -248,24 +247,6 @@ __global__ void k_sym_fill(int32_t N, int64_t nslices, const int32_t* __restrict
   }
 }
 
-// max |v| over an array, reduced into *out as the bit pattern of a
-// non-negative double (whose order is that of the integers).
-__global__ void k_absmax(int64_t n, const double* __restrict__ v, unsigned long long* out) {
-  double m = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    m = fmax(m, fabs(v[i]));
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  __shared__ double sh[32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) sh[w] = m;
-  __syncthreads();
-  if (w == 0) {
-    m = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
-  }
-}
-
 // Copy the upper blocks of the full SELL values into the symmetric storage.
 template <typename TO>
 __global__ void k_sym_pack(int32_t N, const int64_t* __restrict__ sptr, const int64_t* __restrict__ uptr,
@@ -364,7 +345,7 @@ int build_pattern(Ctx* c) {
   if (c->E <= 0 || c->N <= 0) return fail(c, UFC_STATUS_INVALID, "ufc_pattern_build: mesh not set");
   release_graphs(c);
   dfree(&c->uptr); dfree(&c->ucol); dfree(&c->lptr); dfree(&c->lpos); dfree(&c->lcol); dfree(&c->s_lcnt);
-  dfree(&c->sval64); dfree(&c->sval32); dfree(&c->acc);
+  dfree(&c->sval64); dfree(&c->sval32);
   c->has_sym_pattern = c->has_sval64 = c->has_sval32 = false;
   const int32_t N = c->N, E = c->E;
 
@@ -579,20 +560,6 @@ int pack_symmetric(Ctx* c, bool fp64, bool fp32) {
                                                                    c->val64, c->sval64);
     UFC_CUDA(c, cudaGetLastError());
     c->has_sval64 = true;
-  }
-  {
-    // largest stored |K_ij| (the FP32 copy is rounded from these values): with
-    // the longest row it bounds the row sums of the scatter SpMV
-    unsigned long long* w = &c->scal->pmax_bits;
-    UFC_CUDA(c, cudaMemsetAsync(w, 0, sizeof(unsigned long long), c->stream));
-    k_absmax<<<std::min(grid_for(c->sell_blocks * 9, 256), 4096), 256, 0, c->stream>>>(c->sell_blocks * 9, c->val64, w);
-    UFC_CUDA(c, cudaGetLastError());
-    unsigned long long bits = 0;
-    UFC_CUDA(c, cudaMemcpyAsync(&bits, w, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
-    UFC_CUDA(c, cudaStreamSynchronize(c->stream));
-    double m = 0.0;
-    std::memcpy(&m, &bits, sizeof(m));
-    c->sym_absmax = m;
   }
   if (fp32) {
     if (!c->sval32) UFC_TRY(dalloc(c, &c->sval32, nv));

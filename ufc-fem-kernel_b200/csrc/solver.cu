@@ -85,16 +85,6 @@ int vec_grid(int64_t n) {
 
 enum SpmvMode { kPlain = 0, kCg = 1 };
 
-// The CG iterations on symmetric storage use the scatter form of the product
-// (k_spmv_sym_fx) rather than the gather form (k_spmv_sym).
-constexpr bool kScatterSym = true;
-
-// Meshes with fewer than 32 slices per SM run the CG as one persistent
-// cooperative kernel per stretch of iterations (k_cg_persist), at most
-// kPersistSteps iterations per launch.
-constexpr bool kPersistCg = true;
-constexpr int kPersistSteps = 4096;
-
 // The kernels of a CG iteration do nothing once the run has stopped or asked
 // for an FP64 residual replacement: a batch of iterations launched as one graph
 // then idles from the triggering iteration on, so the replacement happens at
@@ -509,118 +499,6 @@ __global__ void __launch_bounds__(kSpmvBlock)
   }
 }
 
-// ---- the symmetric product by scatter, for the CG ----------------------------
-//
-// Each stored upper block K_ij (j > i) is read once and used twice: K_ij x_j
-// for row i (summed in registers by the thread of row i) and K_ij^T x_i for
-// row j, which is added to row j's entry of a fixed-point accumulator with an
-// integer atomic.  Integer addition is associative, so the result does not
-// depend on the order in which the atomics land: the product is deterministic
-// without the lower references and the dependent gathers of k_spmv_sym.
-// Contributions are rounded to integers at the scale 2^e chosen per product
-// from a bound on the partial sums (the largest row length times 3 max|K_ij|
-// times max|x|, times 4), so that every partial sum stays below 2^61 and the
-// rounding step is below 2^-61 of that bound: normwise finer than FP64
-// accumulation of the same row.  The next kernel (k_cg_update in its FX form)
-// reads the accumulator back, scales it, and zeroes it for the next product.
-
-__device__ __forceinline__ void red_add_s64(long long* p, long long v) {
-  asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-// Exponent e of the fixed-point scale 2^e of the current product.  Every
-// kernel that calls it between two updates of pmax_bits sees the same value.
-__device__ __forceinline__ int fx_exponent(const CgScalars* s) {
-  const double pm = __longlong_as_double((long long)s->pmax_bits);
-  const double bound = 4.0 * s->absbound * pm;
-  int e = 0;
-  if (bound > 0.0 && bound <= 1e300) frexp(bound, &e);  // bound < 2^e
-  e = e < -900 ? -900 : e;
-  return 61 - e;
-}
-
-// q = K p (as fixed-point partial sums in acc) with p.q fused and alpha, for
-// the symmetric storage; SPLIT warps per slice on small meshes, each adding its
-// own part of the row sums (no shared-memory combine: the atomics add them).
-template <typename TV, typename TX, typename TA, int SPLIT>
-__global__ void __launch_bounds__(kSpmvBlock)
-    k_spmv_sym_fx(int32_t N, int64_t nslices, const int64_t* __restrict__ uptr, const int32_t* __restrict__ ucol,
-                  const TV* __restrict__ val, const TX* __restrict__ x, long long* __restrict__ acc,
-                  CgScalars* __restrict__ scal, double* __restrict__ partials) {
-  pdl_enter();
-  if (halted(scal)) return;
-  const double sc = ldexp(1.0, fx_exponent(scal));
-  constexpr int kWarps = kSpmvBlock / 32;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int part = warp % SPLIT;
-  const int64_t s = (int64_t)blockIdx.x * (kWarps / SPLIT) + warp / SPLIT;
-  const int64_t row = s * kSlice + lane;
-  double dot[1] = {0.0};
-  if (s < nslices) {
-    const int64_t ub = uptr[s];
-    const int ulen = (int)((uptr[s + 1] - ub) >> 5);
-    const int32_t* ucp = ucol + ub + lane;
-    const TV* uvp = val + 9 * ub + lane;
-    TA xi0 = TA(0), xi1 = TA(0), xi2 = TA(0);
-    if (row < N) {
-      xi0 = (TA)x[3 * row];
-      xi1 = (TA)x[3 * row + 1];
-      xi2 = (TA)x[3 * row + 2];
-    }
-    TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
-    double d = 0.0;
-    auto step = [&](int j) {
-      const int64_t cj = __ldcs(ucp + 32 * j);
-      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
-      const TV* v = uvp + 288 * (int64_t)j;
-      const TA v0 = (TA)__ldcs(v), v1 = (TA)__ldcs(v + 32), v2 = (TA)__ldcs(v + 64);
-      const TA v3 = (TA)__ldcs(v + 96), v4 = (TA)__ldcs(v + 128), v5 = (TA)__ldcs(v + 160);
-      const TA v6 = (TA)__ldcs(v + 192), v7 = (TA)__ldcs(v + 224), v8 = (TA)__ldcs(v + 256);
-      const TA r0 = v0 * x0 + v1 * x1 + v2 * x2;
-      const TA r1 = v3 * x0 + v4 * x1 + v5 * x2;
-      const TA r2 = v6 * x0 + v7 * x1 + v8 * x2;
-      a0 += r0;
-      a1 += r1;
-      a2 += r2;
-      if (cj == row) {  // the diagonal block (or a zero padding block of this row)
-        d += (double)(xi0 * r0 + xi1 * r1 + xi2 * r2);
-      } else {  // (K_ij^T x_i) for row j, and both halves of x_i.K_ij.x_j
-        const TA t0 = v0 * xi0 + v3 * xi1 + v6 * xi2;
-        const TA t1 = v1 * xi0 + v4 * xi1 + v7 * xi2;
-        const TA t2 = v2 * xi0 + v5 * xi1 + v8 * xi2;
-        long long* ap = acc + 3 * cj;
-        red_add_s64(ap, __double2ll_rn((double)t0 * sc));
-        red_add_s64(ap + 1, __double2ll_rn((double)t1 * sc));
-        red_add_s64(ap + 2, __double2ll_rn((double)t2 * sc));
-        d += 2.0 * (double)(t0 * x0 + t1 * x1 + t2 * x2);
-      }
-    };
-    int j = part;
-#pragma unroll 1
-    for (; j + SPLIT < ulen; j += 2 * SPLIT) {
-      step(j);
-      step(j + SPLIT);
-    }
-    for (; j < ulen; j += SPLIT) step(j);
-    if (row < N) {
-      long long* ap = acc + 3 * row;
-      red_add_s64(ap, __double2ll_rn((double)a0 * sc));
-      red_add_s64(ap + 1, __double2ll_rn((double)a1 * sc));
-      red_add_s64(ap + 2, __double2ll_rn((double)a2 * sc));
-    }
-    dot[0] = d;
-  }
-  double tot[1];
-  if (grid_sum<1, sizeof(TV) == 4>(dot, partials, &scal->ticket[0], tot)) {
-    scal->pq = tot[0];
-    if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
-      scal->stop = 3;
-    } else {
-      scal->alpha = scal->rz / tot[0];
-    }
-  }
-}
-
 // 4 consecutive entries through 16-byte loads and stores (cudaMalloc bases are
 // 256-byte aligned; callers pass offsets that are multiples of 4 entries).
 template <typename T>
@@ -644,19 +522,15 @@ __device__ __forceinline__ void st4(T* __restrict__ p, const T (&o)[4]) {
   }
 }
 
-// FX: q is the fixed-point accumulator of k_spmv_sym_fx (read at its scale,
-// then zeroed for the next product); the last block clears max|p| for the
-// direction update that follows.
-template <typename T, bool FX>
+template <typename T>
 __global__ void __launch_bounds__(kVecBlock)
     k_cg_update(int64_t n, const T* __restrict__ p, const T* __restrict__ q, T* __restrict__ r,
                 double* __restrict__ x, const T* __restrict__ dinv, CgScalars* __restrict__ scal,
-                double* __restrict__ partials, long long* __restrict__ acc) {
+                double* __restrict__ partials) {
   pdl_enter();
   if (halted(scal)) return;
   const double alpha = scal->alpha;
   const T a = (T)alpha;
-  const double inv = FX ? ldexp(1.0, -fx_exponent(scal)) : 0.0;
   T rz = T(0), rr = T(0);
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t n4 = n >> 2;
@@ -665,18 +539,7 @@ __global__ void __launch_bounds__(kVecBlock)
     T pv[4], qv[4], rv[4], dv[4];
     double xv[4];
     ld4(p + i, pv);
-    if constexpr (FX) {
-      const longlong2 a01 = *reinterpret_cast<const longlong2*>(acc + i);
-      const longlong2 a23 = *reinterpret_cast<const longlong2*>(acc + i + 2);
-      qv[0] = (T)((double)a01.x * inv);
-      qv[1] = (T)((double)a01.y * inv);
-      qv[2] = (T)((double)a23.x * inv);
-      qv[3] = (T)((double)a23.y * inv);
-      *reinterpret_cast<longlong2*>(acc + i) = make_longlong2(0, 0);
-      *reinterpret_cast<longlong2*>(acc + i + 2) = make_longlong2(0, 0);
-    } else {
-      ld4(q + i, qv);
-    }
+    ld4(q + i, qv);
     ld4(r + i, rv);
     ld4(x + i, xv);
     if (dinv) ld4(dinv + i, dv);
@@ -692,14 +555,7 @@ __global__ void __launch_bounds__(kVecBlock)
     st4(x + i, xv);
   }
   for (int64_t i = (n4 << 2) + gid; i < n; i += stride) {
-    const T pi = p[i];
-    T qi;
-    if constexpr (FX) {
-      qi = (T)((double)acc[i] * inv);
-      acc[i] = 0;
-    } else {
-      qi = q[i];
-    }
+    const T pi = p[i], qi = q[i];
     x[i] += alpha * (double)pi;
     const T ri = r[i] - a * qi;
     r[i] = ri;
@@ -721,33 +577,16 @@ __global__ void __launch_bounds__(kVecBlock)
     else if (!(fabs(rz_old) > 1e-300) || !isfinite(tot[0])) scal->stop = 3;
     else if (it >= scal->max_iter) scal->stop = 2;
     if (scal->delta2 > 0.0 && tot[1] < scal->delta2 * scal->rr_ref) scal->want_update = 1;
-    if (FX) scal->pmax_bits = 0ull;  // every block has read it; k_cg_pupdate refills it
   }
 }
 
-// max |v| over the block, folded into *out (bits of a non-negative double).
-__device__ __forceinline__ void block_absmax_to(double m, unsigned long long* out) {
-  __shared__ double sh[kVecBlock / 32];
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) sh[w] = m;
-  __syncthreads();
-  if (w == 0) {
-    m = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
-  }
-}
-
-// p = D^-1 r + beta p; FX also reduces max|p| for the scale of the next product.
-template <typename T, bool FX>
+template <typename T>
 __global__ void __launch_bounds__(kVecBlock)
     k_cg_pupdate(int64_t n, const T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ p,
-                 CgScalars* __restrict__ scal) {
+                 const CgScalars* __restrict__ scal) {
   pdl_enter();
   if (halted(scal)) return;
   const T beta = (T)scal->beta;
-  double pm = 0.0;
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t n4 = n >> 2;
   for (int64_t k = gid; k < n4; k += stride) {
@@ -757,224 +596,12 @@ __global__ void __launch_bounds__(kVecBlock)
     ld4(p + i, pv);
     if (dinv) ld4(dinv + i, dv);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      pv[c] = (dinv ? dv[c] * rv[c] : rv[c]) + beta * pv[c];
-      if (FX) pm = fmax(pm, fabs((double)pv[c]));
-    }
+    for (int c = 0; c < 4; ++c) pv[c] = (dinv ? dv[c] * rv[c] : rv[c]) + beta * pv[c];
     st4(p + i, pv);
   }
   for (int64_t i = (n4 << 2) + gid; i < n; i += stride) {
     const T ri = r[i];
-    const T pi = (dinv ? dinv[i] * ri : ri) + beta * p[i];
-    p[i] = pi;
-    if (FX) pm = fmax(pm, fabs((double)pi));
-  }
-  if (FX) block_absmax_to(pm, &scal->pmax_bits);
-}
-
-// ---- persistent CG for small meshes -------------------------------------------
-//
-// On meshes with few SELL slices an iteration of three kernels is bound by the
-// launches and the grid-reduction tails, not by bandwidth (212k DOF: about
-// 45 us per iteration, of which the SpMV moves its bytes in 28 us).  This
-// kernel runs the whole iteration loop in one cooperative launch: the SpMV,
-// the update and the direction update are phases separated by grid barriers,
-// and every block sums the per-block partial dot products itself, in block
-// order, so that all blocks take the same scalar decisions with no extra
-// barrier.  It returns when the run stops (converged recursion, maximum
-// iterations, breakdown) or asks for an FP64 residual replacement, exactly
-// where the three-kernel iteration halts, or after max_steps iterations.
-
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Grid barrier (all blocks co-resident by cooperative launch).  bar[0] counts
-// arrivals, bar[1] is the generation.  A wait longer than two seconds sets the
-// device error word and makes every block leave the kernel (returns false).
-__device__ __forceinline__ bool grid_barrier(unsigned int* bar, int32_t* dev_err) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-    volatile unsigned int* gen = bar + 1;
-    const unsigned int g = *gen;
-    __threadfence();
-    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      const unsigned long long t0 = global_ns();
-      while (*gen == g) {
-        if (global_ns() - t0 > 2000000000ull) {
-          atomicOr(dev_err, (int32_t)kDevBarrierTimeout);
-          ok = 0;
-          break;
-        }
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return ok != 0;
-}
-
-// Sum of partials[0..gridDim.x) * NV in block order, identical in every block
-// (warp 0 sums lane-strided, then a fixed shuffle tree); result in all threads.
-template <int NV>
-__device__ __forceinline__ void sum_partials(const double* partials, double (&out)[NV]) {
-  __shared__ double sh[NV];
-  if (threadIdx.x < 32) {
-    double v[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32)
-#pragma unroll
-      for (int k = 0; k < NV; ++k) v[k] += __ldcg(partials + (int64_t)b * NV + k);
-    warp_sum<NV>(v);
-    if (threadIdx.x == 0)
-#pragma unroll
-      for (int k = 0; k < NV; ++k) sh[k] = v[k];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < NV; ++k) out[k] = sh[k];
-  __syncthreads();
-}
-
-template <typename TV, typename TX, typename TA, int SPLIT>
-__global__ void __launch_bounds__(kSpmvBlock)
-    k_cg_persist(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const int32_t* __restrict__ col,
-                 const TV* __restrict__ val, TX* p, TX* q, TX* r, double* x, const TX* __restrict__ dinv, int64_t n,
-                 CgScalars* scal, double* partials, unsigned int* bar, int32_t* dev_err, int max_steps) {
-  constexpr int kWarps = kSpmvBlock / 32, kPer = kWarps / SPLIT;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, part = warp % SPLIT;
-  __shared__ TA sh[kWarps][3][32];
-  double* part_a = partials;                       // [G]     p.q per block
-  double* part_b = partials + gridDim.x;           // [G][2]  r.z, r.r per block
-  if (halted(scal)) return;
-  double rz = scal->rz;
-  const double rr_ref = scal->rr_ref, tol2 = scal->tol2, delta2 = scal->delta2;
-  const int max_iter = scal->max_iter;
-  int iter = scal->iter;
-  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
-  for (int step = 0; step < max_steps; ++step) {
-    // 1. q = K p, p.q
-    double d = 0.0;
-    for (int64_t g = blockIdx.x; g * kPer < nslices; g += gridDim.x) {
-      const int64_t s = g * kPer + warp / SPLIT;
-      const int64_t row = s * kSlice + lane;
-      TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
-      if (s < nslices) {
-        const int64_t base = sptr[s];
-        const int len = (int)((sptr[s + 1] - base) >> 5);
-        const int32_t* cp = col + base + lane;
-        const TV* vp = val + 9 * base + lane;
-#pragma unroll 2
-        for (int j = part; j < len; j += SPLIT) {
-          const int64_t cj = __ldg(cp + 32 * j);
-          const TA x0 = (TA)__ldcg(p + 3 * cj), x1 = (TA)__ldcg(p + 3 * cj + 1), x2 = (TA)__ldcg(p + 3 * cj + 2);
-          const TV* v = vp + 288 * (int64_t)j;
-          a0 += (TA)__ldg(v) * x0 + (TA)__ldg(v + 32) * x1 + (TA)__ldg(v + 64) * x2;
-          a1 += (TA)__ldg(v + 96) * x0 + (TA)__ldg(v + 128) * x1 + (TA)__ldg(v + 160) * x2;
-          a2 += (TA)__ldg(v + 192) * x0 + (TA)__ldg(v + 224) * x1 + (TA)__ldg(v + 256) * x2;
-        }
-      }
-      if constexpr (SPLIT > 1) {
-        sh[warp][0][lane] = a0;
-        sh[warp][1][lane] = a1;
-        sh[warp][2][lane] = a2;
-        __syncthreads();
-        if (part == 0) {
-#pragma unroll
-          for (int k = 1; k < SPLIT; ++k) {
-            a0 += sh[warp + k][0][lane];
-            a1 += sh[warp + k][1][lane];
-            a2 += sh[warp + k][2][lane];
-          }
-        }
-        __syncthreads();
-      }
-      if (part == 0 && s < nslices && row < N) {
-        q[3 * row] = (TX)a0;
-        q[3 * row + 1] = (TX)a1;
-        q[3 * row + 2] = (TX)a2;
-        d += (double)((TA)__ldcg(p + 3 * row) * a0 + (TA)__ldcg(p + 3 * row + 1) * a1 +
-                      (TA)__ldcg(p + 3 * row + 2) * a2);
-      }
-    }
-    {
-      __shared__ double shs[32];
-      double v[1] = {d};
-      block_sum<1>(v, shs);
-      if (threadIdx.x == 0) part_a[blockIdx.x] = v[0];
-    }
-    if (!grid_barrier(bar, dev_err)) return;
-    double pq[1];
-    sum_partials<1>(part_a, pq);
-    if (!(fabs(pq[0]) > 1e-300) || !isfinite(pq[0])) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) {
-        scal->pq = pq[0];
-        scal->stop = 3;
-      }
-      return;
-    }
-    const double alpha = rz / pq[0];
-    const TX a = (TX)alpha;
-    // 2. x += alpha p, r -= alpha q, r.z, r.r
-    TX rzs = TX(0), rrs = TX(0);
-    for (int64_t i = gid; i < n; i += stride) {
-      const TX pi = __ldcg(p + i), qi = __ldcg(q + i);
-      x[i] += alpha * (double)pi;
-      const TX ri = r[i] - a * qi;
-      r[i] = ri;
-      const TX zi = dinv ? dinv[i] * ri : ri;
-      rzs += ri * zi;
-      rrs += ri * ri;
-    }
-    {
-      __shared__ double shs[64];
-      double v[2] = {(double)rzs, (double)rrs};
-      block_sum<2>(v, shs);
-      if (threadIdx.x == 0) {
-        part_b[2 * blockIdx.x] = v[0];
-        part_b[2 * blockIdx.x + 1] = v[1];
-      }
-    }
-    if (!grid_barrier(bar, dev_err)) return;
-    double t[2];
-    sum_partials<2>(part_b, t);
-    const double rz_old = rz, beta = t[0] / rz_old;
-    ++iter;
-    int stop = 0, want = 0;
-    if (t[1] <= tol2) stop = 1;
-    else if (!(fabs(rz_old) > 1e-300) || !isfinite(t[0])) stop = 3;
-    else if (iter >= max_iter) stop = 2;
-    if (delta2 > 0.0 && t[1] < delta2 * rr_ref) want = 1;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      scal->pq = pq[0];
-      scal->alpha = alpha;
-      scal->rz_old = rz_old;
-      scal->rz = t[0];
-      scal->rr = t[1];
-      scal->beta = beta;
-      scal->iter = iter;
-      if (scal->hist && iter <= scal->hist_cap) scal->hist[iter - 1] = t[1];
-      scal->stop = stop;
-      scal->want_update = want;
-    }
-    if (stop || want) return;  // before the direction update, as the three-kernel iteration halts
-    rz = t[0];
-    // 3. p = D^-1 r + beta p
-    const TX b = (TX)beta;
-    for (int64_t i = gid; i < n; i += stride) {
-      const TX ri = r[i];
-      p[i] = (dinv ? dinv[i] * ri : ri) + b * __ldcg(p + i);
-    }
-    if (!grid_barrier(bar, dev_err)) return;
+    p[i] = (dinv ? dinv[i] * ri : ri) + beta * p[i];
   }
 }
 
@@ -1003,10 +630,9 @@ __global__ void __launch_bounds__(kVecBlock)
 template <typename T>
 __global__ void __launch_bounds__(kVecBlock)
     k_replace(int64_t n, const double* __restrict__ res, T* __restrict__ r, const T* __restrict__ dinv,
-              CgScalars* __restrict__ scal, double* __restrict__ partials, int mode, long long* __restrict__ acc) {
+              CgScalars* __restrict__ scal, double* __restrict__ partials, int mode) {
   T rz = T(0), rr = T(0);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    if (acc) acc[i] = 0;  // a product whose update did not run (breakdown) left it dirty
     const T ri = (T)res[i];
     r[i] = ri;
     const T zi = dinv ? dinv[i] * ri : ri;
@@ -1022,7 +648,6 @@ __global__ void __launch_bounds__(kVecBlock)
     scal->rr_ref = tot[1];
     scal->stop = 0;
     scal->want_update = 0;
-    scal->pmax_bits = 0ull;  // refilled by the direction update that follows
   }
 }
 
@@ -1042,7 +667,6 @@ struct Vecs {
   const TV* val;
   const TX* dinv;
   bool sym;
-  long long* acc;  // non-null: the symmetric product in scatter form
 };
 
 template <typename TV, typename TX>
@@ -1062,7 +686,6 @@ Vecs<TV, TX> vecs(Ctx* c, bool precond) {
     v.sym = c->has_sval32;
     v.val = v.sym ? c->sval32 : c->val32;
   }
-  v.acc = v.sym && kScatterSym ? c->acc : nullptr;
   return v;
 }
 
@@ -1089,88 +712,18 @@ void launch_spmv_sym(const Ctx* c, int grid, cudaStream_t st, const TV* val, con
   }
 }
 
-// The scatter product: one warp per slice, or SPLIT warps per slice on small
-// meshes (the rule of spmv_split).
-template <typename TV, typename TX, typename TA>
-void launch_spmv_sym_fx(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, long long* acc) {
-  constexpr int kWarps = kSpmvBlock / 32;
-  auto go = [&](auto kernel, int split) {
-    const int per_block = kWarps / split;
-    const int grid = (int)((c->nslices + per_block - 1) / per_block);
-    launch_pdl(kernel, grid, kSpmvBlock, st, c->N, c->nslices, c->uptr, c->ucol, val, x, acc, c->scal, c->partials);
-  };
-  switch (spmv_split(c)) {
-    case 1: go(k_spmv_sym_fx<TV, TX, TA, 1>, 1); break;
-    case 2: go(k_spmv_sym_fx<TV, TX, TA, 2>, 2); break;
-    case 4: go(k_spmv_sym_fx<TV, TX, TA, 4>, 4); break;
-    default: go(k_spmv_sym_fx<TV, TX, TA, 8>, 8); break;
-  }
-}
-
 template <typename TV, typename TX, typename TA>
 void launch_iteration(const Run& R, const Vecs<TV, TX>& V, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
   Ctx* c = R.c;
   if (ev0) cudaEventRecord(ev0, st);
-  if (V.acc) {
-    launch_spmv_sym_fx<TV, TX, TA>(c, st, V.val, V.p, V.acc);
-  } else if (V.sym) {
+  if (V.sym)
     launch_spmv_sym<TV, TX, TA, kCg>(c, R.sg, st, V.val, V.p, V.q);
-  } else {
+  else
     launch_spmv<TV, TX, TA, kCg>(c, st, V.val, V.p, V.q);
-  }
   if (ev1) cudaEventRecord(ev1, st);
-  if (V.acc) {
-    launch_pdl(k_cg_update<TX, true>, R.vg, kVecBlock, st, R.n, V.p, V.q, V.r, c->x64, V.dinv, c->scal, c->partials,
-               V.acc);
-    launch_pdl(k_cg_pupdate<TX, true>, R.vg, kVecBlock, st, R.n, V.r, V.dinv, V.p, c->scal);
-  } else {
-    launch_pdl(k_cg_update<TX, false>, R.vg, kVecBlock, st, R.n, V.p, V.q, V.r, c->x64, V.dinv, c->scal,
-               c->partials, (long long*)nullptr);
-    launch_pdl(k_cg_pupdate<TX, false>, R.vg, kVecBlock, st, R.n, V.r, V.dinv, V.p, c->scal);
-  }
+  launch_pdl(k_cg_update<TX>, R.vg, kVecBlock, st, R.n, V.p, V.q, V.r, c->x64, V.dinv, c->scal, c->partials);
+  launch_pdl(k_cg_pupdate<TX>, R.vg, kVecBlock, st, R.n, V.r, V.dinv, V.p, c->scal);
   c->launches += 3;
-}
-
-// The persistent CG on full SELL storage: one cooperative launch of up to
-// max_steps iterations, with as many blocks as are co-resident.
-template <typename TV, typename TX, typename TA, int SPLIT>
-int launch_persist_split(const Run& R, const Vecs<TV, TX>& V, int max_steps) {
-  Ctx* c = R.c;
-  auto kernel = k_cg_persist<TV, TX, TA, SPLIT>;
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  UFC_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSpmvBlock, 0));
-  constexpr int kPer = kSpmvBlock / 32 / SPLIT;
-  const int64_t groups = (c->nslices + kPer - 1) / kPer;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, groups));
-  if (3 * (int64_t)grid > c->partials_cap) return fail(c, UFC_STATUS_ERROR, "persistent CG: partial-sum buffer");
-  int32_t N = c->N;
-  int64_t nsl = c->nslices, n = R.n;
-  const int64_t* sptr = c->slice_ptr;
-  const int32_t* col = c->sell_col;
-  const TV* val = V.val;
-  TX *p = V.p, *q = V.q, *r = V.r;
-  double* x = c->x64;
-  const TX* dinv = V.dinv;
-  CgScalars* scal = c->scal;
-  double* partials = c->partials;
-  unsigned int* bar = &c->scal->ticket[6];
-  int32_t* err = c->dev_err;
-  void* args[] = {&N, &nsl, &sptr, &col, &val, &p, &q, &r, &x, &dinv, &n, &scal, &partials, &bar, &err, &max_steps};
-  UFC_CUDA(c, cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(kSpmvBlock), args, 0, c->stream));
-  c->launches += 1;
-  return UFC_STATUS_OK;
-}
-
-template <typename TV, typename TX, typename TA>
-int launch_persist(const Run& R, const Vecs<TV, TX>& V, int max_steps) {
-  switch (spmv_split(R.c)) {
-    case 1: return launch_persist_split<TV, TX, TA, 1>(R, V, max_steps);
-    case 2: return launch_persist_split<TV, TX, TA, 2>(R, V, max_steps);
-    case 4: return launch_persist_split<TV, TX, TA, 4>(R, V, max_steps);
-    default: return launch_persist_split<TV, TX, TA, 8>(R, V, max_steps);
-  }
 }
 
 // FP64 residual of the current x64 into y64 / r-source, true_rr on the device.
@@ -1198,14 +751,11 @@ int true_residual(const Run& R, bool want_bb) {
 template <typename TV, typename TX>
 int replace(const Run& R, const Vecs<TV, TX>& V, int mode) {
   Ctx* c = R.c;
-  k_replace<TX><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, c->y64, V.r, V.dinv, c->scal, c->partials, mode, V.acc);
+  k_replace<TX><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, c->y64, V.r, V.dinv, c->scal, c->partials, mode);
   UFC_CUDA(c, cudaGetLastError());
   c->launches += 1;
   if (mode != 0) {
-    if (V.acc)
-      k_cg_pupdate<TX, true><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, V.r, V.dinv, V.p, c->scal);
-    else
-      k_cg_pupdate<TX, false><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, V.r, V.dinv, V.p, c->scal);
+    k_cg_pupdate<TX><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, V.r, V.dinv, V.p, c->scal);
     UFC_CUDA(c, cudaGetLastError());
     c->launches += 1;
   }
@@ -1228,7 +778,7 @@ int get_graph(const Run& R, const Vecs<TV, TX>& V, int batch, cudaGraphExec_t* o
   // reassembly into the same arrays keeps them
   const void* key = (const void*)V.dinv;
   const void* val = (const void*)V.val;
-  const int form = (V.sym ? 1 : 0) | (c->val32_diff ? 2 : 0) | (V.acc ? 4 : 0);
+  const int form = (V.sym ? 1 : 0) | (c->val32_diff ? 2 : 0);
   if (c->cg_graph[slot] && c->cg_graph_batch[slot] == batch && c->cg_graph_key[slot] == key &&
       c->cg_graph_val[slot] == val && c->cg_graph_form[slot] == form) {
     *out = c->cg_graph[slot];
@@ -1275,10 +825,6 @@ int ensure_vectors(Ctx* c, int prec) {
     UFC_TRY(need(&c->q32));
   }
   if (prec != UFC_PRECISION_FP64) UFC_TRY(need(&c->xb64));
-  if (kScatterSym && c->has_sym_pattern && !c->acc) {
-    UFC_TRY(need(&c->acc));
-    UFC_CUDA(c, cudaMemsetAsync(c->acc, 0, sizeof(long long) * n, c->stream));
-  }
   if (realloc) release_graphs(c);
   return UFC_STATUS_OK;
 }
@@ -1304,8 +850,6 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
   CgScalars h{};
   h.max_iter = algo->max_iter > 0 ? algo->max_iter : 1;
   h.delta2 = 0.0;
-  // |any partial row sum of the scatter product| <= absbound * max|p|
-  h.absbound = 3.0 * (double)c->max_row_blocks * c->sym_absmax * (1.0 + 1e-6);
   if (prec != UFC_PRECISION_FP64) {
     const double d = algo->refine_delta > 0.0 ? algo->refine_delta : 0.1;
     h.delta2 = d * d;
@@ -1337,10 +881,8 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
     double tol2 = tol * tol;
     UFC_CUDA(c, cudaMemcpyAsync(&c->scal->tol2, &tol2, sizeof(double), cudaMemcpyHostToDevice, c->stream));
     UFC_TRY(replace(R, V, 2));
-    // small meshes (few slices per SM) on full storage: the persistent CG
-    const bool persist = kPersistCg && !V.sym && !c->val32_diff && !c->instrument && spmv_split(c) > 1;
     cudaGraphExec_t graph = nullptr;
-    if (!c->instrument && !persist) UFC_TRY((get_graph<TV, TX, TA>(R, V, batch, &graph)));
+    if (!c->instrument) UFC_TRY((get_graph<TV, TX, TA>(R, V, batch, &graph)));
     std::vector<cudaEvent_t> evs;
     if (c->instrument) {
       evs.resize(2 * batch);
@@ -1361,10 +903,7 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
     bool finished = false;
     int status = UFC_STATUS_OK;
     while (!finished) {
-      if (persist) {
-        status = launch_persist<TV, TX, TA>(R, V, kPersistSteps);
-        if (status != UFC_STATUS_OK) break;
-      } else if (graph) {
+      if (graph) {
         cudaError_t e = cudaGraphLaunch(graph, c->stream);
         if (e != cudaSuccess) {
           status = cuda_fail(c, e, "cudaGraphLaunch");
@@ -1510,12 +1049,9 @@ int64_t spmv_bytes(const Ctx* c, int precision) {
   const int64_t sx = precision == UFC_PRECISION_FP32_REFINE ? 4 : 8;  // vector entry
   const bool sym = precision == UFC_PRECISION_FP64 ? c->has_sval64 : c->has_sval32;
   if (sym) {
+    // symmetric storage: upper blocks (values + column), lower references
+    // (position + column; their values are re-read from L2), x and y
     const int64_t upper = (c->nnzb + c->N) / 2, lower = (c->nnzb - c->N) / 2;
-    // scatter form: upper blocks (values + column), x read, and the 8-byte
-    // fixed-point accumulator of y written
-    if (kScatterSym) return upper * (9 * sv + 4) + c->n * sx + c->n * 8;
-    // gather form: upper blocks, lower references (position + column; their
-    // values are re-read from L2), x and y
     return upper * (9 * sv + 4) + lower * 8 + 2 * c->n * sx;
   }
   return c->nnzb * (9 * sv + 4) + 4 * ((int64_t)c->N + 1) + 2 * c->n * sx;

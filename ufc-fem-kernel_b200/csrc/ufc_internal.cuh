@@ -38,11 +38,6 @@ struct CgScalars {
   int32_t max_iter;
   int32_t stop;     // 1 converged (recursive), 2 max-iter, 3 breakdown
   int32_t want_update;
-  // scatter form of the symmetric SpMV: bits of max|p| (a non-negative double,
-  // reduced by atomicMax on its bit pattern) and the bound on |K| row sums,
-  // which together fix the fixed-point scale of the product
-  unsigned long long pmax_bits;
-  double absbound;
   double nr_rr, nr_ff, nr_ee;  // Newton: ||R_free||^2, ||F_int||^2, ||F_ext||^2
   double* hist;        // ||r||^2 of the recursive residual per iteration (or null)
   int32_t hist_cap;
@@ -57,7 +52,6 @@ enum DevErr : int32_t {
   kDevValence = 4,
   kDevRowBlocks = 8,
   kDevPattern = 16,
-  kDevBarrierTimeout = 32,
 };
 
 struct Mg;  // multigrid hierarchy (mg.cu)
@@ -122,8 +116,6 @@ struct Ctx {
   double* sval64 = nullptr;              // [(s_ublocks + 32) * 9]
   float* sval32 = nullptr;
   bool has_sval64 = false, has_sval32 = false;
-  double sym_absmax = 0.0;               // max |K_ij| over the stored values
-  long long* acc = nullptr;              // [n] fixed-point accumulator of the scatter SpMV (zero between uses)
 
   // Dirichlet set
   uint8_t* fixed = nullptr;  // [n]
