@@ -774,6 +774,9 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* Bm, double* X, const ufc_sol
   BTRY(dalloc(c, &B.xx, B.nn));
   BTRY(dalloc(c, &B.rx, B.nn));
   BTRY(dalloc(c, &B.px, B.nn));
+  // columns that never restart (padding, or converged at the start) are
+  // multiplied by alpha = 0: they must hold numbers, not whatever was there
+  BCUDA(cudaMemsetAsync(B.px, 0, sizeof(double) * B.nn, c->stream));
   BTRY(dalloc(c, &B.qx, B.nn));
   BTRY(dalloc(c, &B.s, 1));
   BTRY(dalloc(c, &B.partials, (int64_t)std::max(B.g_spmv, B.g_vec) * kNvMax * kMaxRhs));

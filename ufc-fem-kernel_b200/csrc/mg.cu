@@ -448,8 +448,9 @@ __global__ void k_mgcg_pupdate(int64_t n, const double* __restrict__ z, double* 
                                const CgScalars* __restrict__ scal) {
   if (scal->stop) return;
   const double b = scal->beta;
+  // beta = 0 (start, restart): p = z without reading p, which may hold anything
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = z[i] + b * p[i];
+    p[i] = b == 0.0 ? z[i] : z[i] + b * p[i];
 }
 
 // ---------------------------------------------------------------- host side

@@ -587,13 +587,16 @@ __global__ void __launch_bounds__(kVecBlock)
   pdl_enter();
   if (halted(scal)) return;
   const T beta = (T)scal->beta;
+  // beta = 0 (start, restart after a breakdown): p = z without reading p, whose
+  // contents are then undefined (fresh memory, or the NaN of the breakdown)
+  const bool fresh = scal->beta == 0.0;
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t n4 = n >> 2;
   for (int64_t k = gid; k < n4; k += stride) {
     const int64_t i = k << 2;
-    T rv[4], pv[4], dv[4];
+    T rv[4], pv[4] = {T(0), T(0), T(0), T(0)}, dv[4];
     ld4(r + i, rv);
-    ld4(p + i, pv);
+    if (!fresh) ld4(p + i, pv);
     if (dinv) ld4(dinv + i, dv);
 #pragma unroll
     for (int c = 0; c < 4; ++c) pv[c] = (dinv ? dv[c] * rv[c] : rv[c]) + beta * pv[c];
@@ -601,7 +604,7 @@ __global__ void __launch_bounds__(kVecBlock)
   }
   for (int64_t i = (n4 << 2) + gid; i < n; i += stride) {
     const T ri = r[i];
-    p[i] = (dinv ? dinv[i] * ri : ri) + beta * p[i];
+    p[i] = (dinv ? dinv[i] * ri : ri) + (fresh ? T(0) : beta * p[i]);
   }
 }
 
