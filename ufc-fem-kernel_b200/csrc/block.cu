@@ -657,7 +657,7 @@ static int pcg_block_run(BlockRun& B, int nrhs, const ufc_solver_algo* algo, BSc
   for (int k = 0; k < nr; ++k) {
     const double bn = std::sqrt(hs->bb[k]);
     bnorm[k] = bn < 1e-30 ? 1.0 : bn;
-    tol[k] = kStopMargin * std::max(algo->tolerance * bnorm[k], algo->abs_tolerance);
+    tol[k] = std::max(algo->tolerance * bnorm[k], algo->abs_tolerance);
     if (k < nrhs) st[k].initial_residual = std::sqrt(hs->true_rr[k]);
   }
   const int batch = algo->check_every > 0 ? algo->check_every : 32;

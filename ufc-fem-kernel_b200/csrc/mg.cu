@@ -936,7 +936,7 @@ int pcg_mg(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
     return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: non-finite initial residual (initial guess or matrix)");
   const double bnorm_raw = std::sqrt(c->h_scal->bb);
   const double bnorm = bnorm_raw < 1e-30 ? 1.0 : bnorm_raw;
-  const double tol = kStopMargin * std::max(algo->tolerance * bnorm, algo->abs_tolerance);
+  const double tol = std::max(algo->tolerance * bnorm, algo->abs_tolerance);
   st->initial_residual = std::sqrt(c->h_scal->true_rr);
   double true_rr = c->h_scal->true_rr;
   bool converged = std::sqrt(true_rr) <= tol;

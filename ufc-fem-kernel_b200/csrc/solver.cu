@@ -932,7 +932,8 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
     return fail(c, UFC_STATUS_INVALID, "ufc_pcg_solve: non-finite initial residual (initial guess or matrix)");
   const double bnorm_raw = std::sqrt(c->h_scal->bb);
   const double bnorm = bnorm_raw < 1e-30 ? 1.0 : bnorm_raw;
-  const double tol = kStopMargin * std::max(algo->tolerance * bnorm, algo->abs_tolerance);
+  const double tol_nominal = std::max(algo->tolerance * bnorm, algo->abs_tolerance);
+  const double tol = kStopMargin * tol_nominal;
   st->initial_residual = std::sqrt(c->h_scal->true_rr);
   double true_rr = c->h_scal->true_rr;
   int flag = 0;
@@ -1071,6 +1072,11 @@ int pcg_run(Ctx* c, const ufc_solver_algo* algo, ufc_solver_state* st) {
     cudaEventDestroy(done[0]);
     cudaEventDestroy(done[1]);
     if (status != UFC_STATUS_OK) return status;
+    // stalled or out of iterations short of the margin, but within the tolerance
+    if (!converged && std::isfinite(true_rr) && std::sqrt(true_rr) <= tol_nominal) {
+      converged = true;
+      flag = 0;
+    }
   }
   UFC_TRY(read_scalars(c));
   UFC_CUDA(c, cudaEventRecord(t1, c->stream));
