@@ -140,7 +140,6 @@ void free_all(Ctx* c) {
   dfree(&c->fixed); dfree(&c->fix_dofs); dfree(&c->fix_vals);
   dfree(&c->x64); dfree(&c->r64); dfree(&c->p64); dfree(&c->q64); dfree(&c->b64); dfree(&c->y64);
   dfree(&c->r32); dfree(&c->p32); dfree(&c->q32); dfree(&c->xb64); dfree(&c->hist);
-  dfree(&c->p4_32); dfree(&c->p4_64);
   c->hist_cap = c->hist_len = 0;
   dfree(&c->nr_fint); dfree(&c->nr_R); dfree(&c->nr_du); dfree(&c->nr_dc);
   dfree(&c->u); dfree(&c->u_n);

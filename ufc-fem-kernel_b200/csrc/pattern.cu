@@ -345,7 +345,7 @@ int build_pattern(Ctx* c) {
   if (c->E <= 0 || c->N <= 0) return fail(c, UFC_STATUS_INVALID, "ufc_pattern_build: mesh not set");
   release_graphs(c);
   dfree(&c->uptr); dfree(&c->ucol); dfree(&c->lptr); dfree(&c->lpos); dfree(&c->lcol); dfree(&c->s_lcnt);
-  dfree(&c->sval64); dfree(&c->sval32); dfree(&c->p4_32); dfree(&c->p4_64);
+  dfree(&c->sval64); dfree(&c->sval32);
   c->has_sym_pattern = c->has_sval64 = c->has_sval32 = false;
   const int32_t N = c->N, E = c->E;
 

@@ -85,10 +85,6 @@ int vec_grid(int64_t n) {
 
 enum SpmvMode { kPlain = 0, kCg = 1 };
 
-// The symmetric CG product gathers p from a node-padded copy (k_cg_pupdate
-// writes it beside p).
-constexpr bool kPaddedP = true;
-
 // The kernels of a CG iteration do nothing once the run has stopped or asked
 // for an FP64 residual replacement: a batch of iterations launched as one graph
 // then idles from the triggering iteration on, so the replacement happens at
@@ -313,33 +309,13 @@ __device__ __forceinline__ void sym_prefetch(int lane, int k1, int ulen, int lle
   }
 }
 
-// The three components of node j of x: X4 = false, x in DOF order (three
-// 4- or 8-byte loads at 3j); X4 = true, x node-padded to four entries per node
-// (one 16-byte load for FP32, two for FP64), the copy of p that
-// k_cg_pupdate writes for the CG products.
-template <bool X4, typename TA, typename TX>
-__device__ __forceinline__ void gather3(const TX* __restrict__ x, int64_t j, TA& x0, TA& x1, TA& x2) {
-  if constexpr (X4) {
-    if constexpr (sizeof(TX) == 4) {
-      const float4 v = __ldg(reinterpret_cast<const float4*>(x) + j);
-      x0 = (TA)v.x; x1 = (TA)v.y; x2 = (TA)v.z;
-    } else {
-      const double2 a = __ldg(reinterpret_cast<const double2*>(x) + 2 * j);
-      const double2 b = __ldg(reinterpret_cast<const double2*>(x) + 2 * j + 1);
-      x0 = (TA)a.x; x1 = (TA)a.y; x2 = (TA)b.x;
-    }
-  } else {
-    x0 = (TA)__ldg(x + 3 * j); x1 = (TA)__ldg(x + 3 * j + 1); x2 = (TA)__ldg(x + 3 * j + 2);
-  }
-}
-
 // y = K x from the symmetric storage: row i sums its upper blocks K_ij x_j
 // (j >= i, SELL-32, coalesced) and its lower blocks as transposes K_ji^T x_j of
 // the blocks stored by the earlier rows j.  Those transposed reads are from
 // blocks streamed by rows at most about one node plane earlier, so they come
 // from L2; the upper values are loaded with the default cache policy so that
 // they stay there.
-template <typename TV, typename TX, typename TA, int MODE, bool X4>
+template <typename TV, typename TX, typename TA, int MODE>
 __global__ void __launch_bounds__(kSpmvBlock)
     k_spmv_sym(int32_t N, int64_t nrows_pad, const int64_t* __restrict__ uptr, const int32_t* __restrict__ ucol,
                const int64_t* __restrict__ lptr, const int32_t* __restrict__ lpos, const int32_t* __restrict__ lcol,
@@ -365,8 +341,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
     // branches so that the loads of both halves are in flight together
     auto upper = [&](int j) {
       const int64_t cj = __ldcs(ucp + 32 * j);
-      TA x0, x1, x2;
-      gather3<X4>(x, cj, x0, x1, x2);
+      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
       const TV* v = uvp + 288 * (int64_t)j;
       a0 += (TA)v[0] * x0 + (TA)v[32] * x1 + (TA)v[64] * x2;
       a1 += (TA)v[96] * x0 + (TA)v[128] * x1 + (TA)v[160] * x2;
@@ -375,8 +350,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
     auto lower = [&](int j) {
       const int64_t P = __ldcs(lpp + 32 * j);
       const int64_t cj = __ldcs(lcp + 32 * j);
-      TA x0, x1, x2;
-      gather3<X4>(x, cj, x0, x1, x2);
+      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
       const TV* v = val + 9 * (P & ~int64_t(31)) + (P & 31);
       // transposed block: (K_ji^T x)_r = sum_c K_ji[c][r] x_c
       a0 += (TA)__ldg(v) * x0 + (TA)__ldg(v + 96) * x1 + (TA)__ldg(v + 192) * x2;
@@ -420,10 +394,8 @@ __global__ void __launch_bounds__(kSpmvBlock)
       y[3 * row] = (TX)a0;
       y[3 * row + 1] = (TX)a1;
       y[3 * row + 2] = (TX)a2;
-      if (MODE == kCg) {
-        constexpr int kS = X4 ? 4 : 3;
-        dot[0] = (double)((TA)x[kS * row] * a0 + (TA)x[kS * row + 1] * a1 + (TA)x[kS * row + 2] * a2);
-      }
+      if (MODE == kCg)
+        dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
     }
   }
   if (MODE == kCg) {
@@ -443,7 +415,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
 // slices to fill the GPU one warp each: warp `part` of a slice takes the
 // upper and lower steps j = part, part + SPLIT, ..., and the row sums of the
 // slice's warps are added in shared memory in warp order.
-template <typename TV, typename TX, typename TA, int MODE, int SPLIT, bool X4>
+template <typename TV, typename TX, typename TA, int MODE, int SPLIT>
 __global__ void __launch_bounds__(kSpmvBlock)
     k_spmv_sym_split(int32_t N, int64_t nslices, const int64_t* __restrict__ uptr, const int32_t* __restrict__ ucol,
                      const int64_t* __restrict__ lptr, const int32_t* __restrict__ lpos,
@@ -467,8 +439,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
     const int32_t* lcp = lcol + lb + lane;
     auto upper = [&](int j) {
       const int64_t cj = __ldcs(ucp + 32 * j);
-      TA x0, x1, x2;
-      gather3<X4>(x, cj, x0, x1, x2);
+      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
       const TV* v = uvp + 288 * (int64_t)j;
       a0 += (TA)v[0] * x0 + (TA)v[32] * x1 + (TA)v[64] * x2;
       a1 += (TA)v[96] * x0 + (TA)v[128] * x1 + (TA)v[160] * x2;
@@ -477,8 +448,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
     auto lower = [&](int j) {
       const int64_t P = __ldcs(lpp + 32 * j);
       const int64_t cj = __ldcs(lcp + 32 * j);
-      TA x0, x1, x2;
-      gather3<X4>(x, cj, x0, x1, x2);
+      const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
       const TV* v = val + 9 * (P & ~int64_t(31)) + (P & 31);
       a0 += (TA)__ldg(v) * x0 + (TA)__ldg(v + 96) * x1 + (TA)__ldg(v + 192) * x2;
       a1 += (TA)__ldg(v + 32) * x0 + (TA)__ldg(v + 128) * x1 + (TA)__ldg(v + 224) * x2;
@@ -514,10 +484,7 @@ __global__ void __launch_bounds__(kSpmvBlock)
     y[3 * row] = (TX)a0;
     y[3 * row + 1] = (TX)a1;
     y[3 * row + 2] = (TX)a2;
-    if (MODE == kCg) {
-      constexpr int kS = X4 ? 4 : 3;
-      dot[0] = (double)((TA)x[kS * row] * a0 + (TA)x[kS * row + 1] * a1 + (TA)x[kS * row + 2] * a2);
-    }
+    if (MODE == kCg) dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
   }
   if (MODE == kCg) {
     double tot[1];
@@ -616,7 +583,7 @@ __global__ void __launch_bounds__(kVecBlock)
 template <typename T>
 __global__ void __launch_bounds__(kVecBlock)
     k_cg_pupdate(int64_t n, const T* __restrict__ r, const T* __restrict__ dinv, T* __restrict__ p,
-                 const CgScalars* __restrict__ scal, T* __restrict__ p4) {
+                 const CgScalars* __restrict__ scal) {
   pdl_enter();
   if (halted(scal)) return;
   const T beta = (T)scal->beta;
@@ -634,16 +601,10 @@ __global__ void __launch_bounds__(kVecBlock)
 #pragma unroll
     for (int c = 0; c < 4; ++c) pv[c] = (dinv ? dv[c] * rv[c] : rv[c]) + beta * pv[c];
     st4(p + i, pv);
-    if (p4) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) p4[((i + c) / 3) * 4 + (i + c) % 3] = pv[c];
-    }
   }
   for (int64_t i = (n4 << 2) + gid; i < n; i += stride) {
     const T ri = r[i];
-    const T pi = (dinv ? dinv[i] * ri : ri) + (fresh ? T(0) : beta * p[i]);
-    p[i] = pi;
-    if (p4) p4[(i / 3) * 4 + i % 3] = pi;
+    p[i] = (dinv ? dinv[i] * ri : ri) + (fresh ? T(0) : beta * p[i]);
   }
 }
 
@@ -706,7 +667,6 @@ struct Run {
 template <typename TV, typename TX>
 struct Vecs {
   TX *r, *p, *q;
-  TX* p4;  // node-padded copy of p for the symmetric product (or null)
   const TV* val;
   const TX* dinv;
   bool sym;
@@ -729,34 +689,29 @@ Vecs<TV, TX> vecs(Ctx* c, bool precond) {
     v.sym = c->has_sval32;
     v.val = v.sym ? c->sval32 : c->val32;
   }
-  if constexpr (sizeof(TX) == 8)
-    v.p4 = v.sym && kPaddedP ? c->p4_64 : nullptr;
-  else
-    v.p4 = v.sym && kPaddedP ? c->p4_32 : nullptr;
   return v;
 }
 
-template <typename TV, typename TX, typename TA, int MODE, int SPLIT, bool X4>
+template <typename TV, typename TX, typename TA, int MODE, int SPLIT>
 void launch_spmv_sym_split(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
   constexpr int per_block = kSpmvBlock / 32 / SPLIT;
   const int grid = (int)((c->nslices + per_block - 1) / per_block);
-  launch_mode<MODE>(k_spmv_sym_split<TV, TX, TA, MODE, SPLIT, X4>, grid, kSpmvBlock, st, c->N, c->nslices, c->uptr,
+  launch_mode<MODE>(k_spmv_sym_split<TV, TX, TA, MODE, SPLIT>, grid, kSpmvBlock, st, c->N, c->nslices, c->uptr,
                     c->ucol, c->lptr, c->lpos, c->lcol, val, x, y, c->scal, c->partials);
 }
 
 // The symmetric product: one warp per slice (grid = slices / 8 blocks), or
 // SPLIT warps per slice on small meshes (the rule of spmv_split).
-// X4: x is node-padded (four entries per node).
-template <typename TV, typename TX, typename TA, int MODE, bool X4 = false>
+template <typename TV, typename TX, typename TA, int MODE>
 void launch_spmv_sym(const Ctx* c, int grid, cudaStream_t st, const TV* val, const TX* x, TX* y) {
   switch (spmv_split(c)) {
     case 1:
-      launch_mode<MODE>(k_spmv_sym<TV, TX, TA, MODE, X4>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice, c->uptr,
+      launch_mode<MODE>(k_spmv_sym<TV, TX, TA, MODE>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice, c->uptr,
                         c->ucol, c->lptr, c->lpos, c->lcol, val, x, y, c->scal, c->partials);
       break;
-    case 2: launch_spmv_sym_split<TV, TX, TA, MODE, 2, X4>(c, st, val, x, y); break;
-    case 4: launch_spmv_sym_split<TV, TX, TA, MODE, 4, X4>(c, st, val, x, y); break;
-    default: launch_spmv_sym_split<TV, TX, TA, MODE, 8, X4>(c, st, val, x, y); break;
+    case 2: launch_spmv_sym_split<TV, TX, TA, MODE, 2>(c, st, val, x, y); break;
+    case 4: launch_spmv_sym_split<TV, TX, TA, MODE, 4>(c, st, val, x, y); break;
+    default: launch_spmv_sym_split<TV, TX, TA, MODE, 8>(c, st, val, x, y); break;
   }
 }
 
@@ -764,15 +719,13 @@ template <typename TV, typename TX, typename TA>
 void launch_iteration(const Run& R, const Vecs<TV, TX>& V, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1) {
   Ctx* c = R.c;
   if (ev0) cudaEventRecord(ev0, st);
-  if (V.sym && V.p4)
-    launch_spmv_sym<TV, TX, TA, kCg, true>(c, R.sg, st, V.val, V.p4, V.q);
-  else if (V.sym)
+  if (V.sym)
     launch_spmv_sym<TV, TX, TA, kCg>(c, R.sg, st, V.val, V.p, V.q);
   else
     launch_spmv<TV, TX, TA, kCg>(c, st, V.val, V.p, V.q);
   if (ev1) cudaEventRecord(ev1, st);
   launch_pdl(k_cg_update<TX>, R.vg, kVecBlock, st, R.n, V.p, V.q, V.r, c->x64, V.dinv, c->scal, c->partials);
-  launch_pdl(k_cg_pupdate<TX>, R.vg, kVecBlock, st, R.n, V.r, V.dinv, V.p, c->scal, V.p4);
+  launch_pdl(k_cg_pupdate<TX>, R.vg, kVecBlock, st, R.n, V.r, V.dinv, V.p, c->scal);
   c->launches += 3;
 }
 
@@ -805,7 +758,7 @@ int replace(const Run& R, const Vecs<TV, TX>& V, int mode) {
   UFC_CUDA(c, cudaGetLastError());
   c->launches += 1;
   if (mode != 0) {
-    k_cg_pupdate<TX><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, V.r, V.dinv, V.p, c->scal, V.p4);
+    k_cg_pupdate<TX><<<R.vg, kVecBlock, 0, c->stream>>>(R.n, V.r, V.dinv, V.p, c->scal);
     UFC_CUDA(c, cudaGetLastError());
     c->launches += 1;
   }
@@ -828,7 +781,7 @@ int get_graph(const Run& R, const Vecs<TV, TX>& V, int batch, cudaGraphExec_t* o
   // reassembly into the same arrays keeps them
   const void* key = (const void*)V.dinv;
   const void* val = (const void*)V.val;
-  const int form = (V.sym ? 1 : 0) | (c->val32_diff ? 2 : 0) | (V.p4 ? 4 : 0);
+  const int form = (V.sym ? 1 : 0) | (c->val32_diff ? 2 : 0);
   if (c->cg_graph[slot] && c->cg_graph_batch[slot] == batch && c->cg_graph_key[slot] == key &&
       c->cg_graph_val[slot] == val && c->cg_graph_form[slot] == form) {
     *out = c->cg_graph[slot];
@@ -875,18 +828,6 @@ int ensure_vectors(Ctx* c, int prec) {
     UFC_TRY(need(&c->q32));
   }
   if (prec != UFC_PRECISION_FP64) UFC_TRY(need(&c->xb64));
-  if (kPaddedP && c->has_sym_pattern) {
-    const int64_t n4 = 4 * (int64_t)c->N;
-    if (prec == UFC_PRECISION_FP64 || prec == UFC_PRECISION_FP32_MATRIX) {
-      if (!c->p4_64) {
-        realloc = true;
-        UFC_TRY(dalloc(c, &c->p4_64, n4));
-      }
-    } else if (!c->p4_32) {
-      realloc = true;
-      UFC_TRY(dalloc(c, &c->p4_32, n4));
-    }
-  }
   if (realloc) release_graphs(c);
   return UFC_STATUS_OK;
 }

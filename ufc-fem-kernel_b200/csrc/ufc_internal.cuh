@@ -130,10 +130,6 @@ struct Ctx {
   // solver work
   double *x64 = nullptr, *r64 = nullptr, *p64 = nullptr, *q64 = nullptr, *b64 = nullptr, *y64 = nullptr;
   float *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
-  // node-padded copies of p (four entries per node) that the symmetric CG
-  // product gathers with one 16-byte load per node (FP32) or two (FP64)
-  float* p4_32 = nullptr;
-  double* p4_64 = nullptr;
   double* xb64 = nullptr;  // best iterate of an FP32 run (handed to the FP64 continuation)
   CgScalars* scal = nullptr;
   double* hist = nullptr;       // residual history of the last solve (device)
