@@ -276,3 +276,37 @@ def test_elimination_matches_reference_penalty(pkg, orc):
     u, st = m.solve(pkg.lifted_rhs(m, p.f), pkg.SolverAlgo(tolerance=1e-12))
     u_pen = _penalty_solution(p, orc.Model(p).assemble(eliminate=False))
     assert st.converged and np.linalg.norm(u - u_pen) / np.linalg.norm(u_pen) <= 1e-9
+
+
+def test_symmetric_coded_indices_large_mesh(pkg, orc):
+    """A mesh with more than 32 slices per SM takes the symmetric product with
+    coded indices (per row 16 upper and 16 lower code bytes instead of 4-byte
+    columns and lower references; stencil-like patterns only): its products in
+    FP64 and FP32 against the oracle's CSR, a refined FP32 solve and an FP64
+    solve against the full storage, and the bytes per product it reports."""
+    p = pkg.mesh.lognormal_cantilever(64, 48, 48, seed=8)
+    sym = _model(pkg, p, pkg.BUILD_FP64 | pkg.BUILD_FP32_ROUNDED | pkg.BUILD_SYMMETRIC)
+    full = _model(pkg, p, pkg.BUILD_FP64 | pkg.BUILD_FP32_ROUNDED)
+    K = orc.Model(p).assemble()
+    x = np.random.default_rng(3).standard_normal(p.n_dof)
+    y_o = K.matvec(x)
+    scale = np.abs(y_o).max()
+    assert np.abs(sym.spmv(x) - y_o).max() <= 1e-13 * scale
+    x32 = x.astype(np.float32)
+    assert np.abs(sym.spmv(x32, precision=pkg.PRECISION_FP32_REFINE) - y_o).max() <= 1e-5 * scale
+    b = pkg.lifted_rhs(sym, p.f)
+    for prec in (pkg.PRECISION_FP64, pkg.PRECISION_FP32_REFINE):
+        algo = pkg.SolverAlgo(tolerance=1e-10, precision_mode=prec)
+        us, ss = sym.solve(b, algo)
+        uf, sf = full.solve(b, algo)
+        assert ss.converged and sf.converged
+        assert np.linalg.norm(us - uf) / np.linalg.norm(uf) <= 1e-9
+    # the coded form reports its own bytes: 9 s per upper block + 32 code bytes per row + x and y
+    sym.set_instrument(True)
+    sym.solve(b, pkg.SolverAlgo(tolerance=1e-10))
+    t = sym.last_timing()
+    sym.set_instrument(False)
+    info = sym.info
+    nrows = (p.n_nodes + 31) // 32 * 32
+    upper = (info.nnzb + p.n_nodes) // 2
+    assert t["spmv_bytes"] == upper * 72 + 32 * nrows + 16 * p.n_dof

@@ -247,6 +247,74 @@ __global__ void k_sym_fill(int32_t N, int64_t nslices, const int32_t* __restrict
   }
 }
 
+// Coded indices of the symmetric storage.  First the set of upper offsets
+// (col - row >= 0) of the real blocks, as bits of a bitmap over [0, kOffRange);
+// a larger offset sets bit 0 of *flags (the pattern is not stencil-like).
+constexpr int64_t kOffRange = 1 << 21;
+
+__global__ void k_sym_offsets(int32_t N, int64_t nslices, const int64_t* __restrict__ uptr,
+                              const int32_t* __restrict__ ucol, uint32_t* __restrict__ bits,
+                              int32_t* __restrict__ flags) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
+  const int64_t s = r / kSlice, t = r % kSlice;
+  const int64_t ub = uptr[s], ul = (uptr[s + 1] - ub) / kSlice;
+  if (ul > 16) atomicOr(flags, 2);
+  for (int64_t k = 0; k < ul; ++k) {
+    const int64_t c = ucol[ub + k * kSlice + t];
+    if (k > 0 && c == r) continue;  // padding
+    const int64_t d = c - r;
+    if (d < 0 || d >= kOffRange) {
+      atomicOr(flags, 1);
+      continue;
+    }
+    atomicOr(bits + (d >> 5), 1u << (d & 31));
+  }
+}
+
+// The code bytes, lane-major: row r's 16 upper codes at ucode[16 r], its 16
+// lower codes at lcode[16 r].  Upper code: index of col - row in tab (15: no
+// block, the padding).  Lower code: (index of row - col) << 4 | rank of the
+// block (col, row) in row col's upper list (0xFF: no block).  Sets bit 2 of
+// *flags when a slice has more than 16 lower steps or an offset is not in tab.
+__global__ void k_sym_codes(int32_t N, int64_t nslices, const int64_t* __restrict__ uptr,
+                            const int64_t* __restrict__ lptr, const int32_t* __restrict__ ucol,
+                            const int32_t* __restrict__ lpos, const int32_t* __restrict__ lcol, int64_t zero_pos,
+                            SymOffsets tab, int ntab, uint8_t* __restrict__ ucode, uint8_t* __restrict__ lcode,
+                            int32_t* __restrict__ flags) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nslices * kSlice) return;
+  const int64_t s = r / kSlice, t = r % kSlice;
+  const int64_t ub = uptr[s], ul = (uptr[s + 1] - ub) / kSlice;
+  const int64_t lb = lptr[s], ll = (lptr[s + 1] - lb) / kSlice;
+  if (ll > 16 || ul > 16) atomicOr(flags, 4);
+  auto find = [&](int64_t d) -> int {
+    for (int q = 0; q < ntab; ++q)
+      if (tab.off[q] == d) return q;
+    atomicOr(flags, 4);
+    return kSymCodes;
+  };
+  for (int k = 0; k < 16; ++k) {
+    uint8_t u = kSymCodes, l = 0xFF;
+    if (r < N && k < ul) {
+      const int64_t c = ucol[ub + k * kSlice + t];
+      if (k == 0 || c != r) u = (uint8_t)find(c - r);
+    }
+    if (r < N && k < ll) {
+      const int64_t pos = lpos[lb + k * kSlice + t];
+      if (pos != zero_pos) {
+        const int64_t c = lcol[lb + k * kSlice + t];
+        const int64_t rank = (pos - uptr[c / kSlice] - c % kSlice) / kSlice;
+        const int q = find(r - c);
+        if (rank < 0 || rank > 15 || q >= kSymCodes) atomicOr(flags, 4);
+        else l = (uint8_t)((q << 4) | rank);
+      }
+    }
+    ucode[r * 16 + k] = u;
+    lcode[r * 16 + k] = l;
+  }
+}
+
 // Copy the upper blocks of the full SELL values into the symmetric storage.
 template <typename TO>
 __global__ void k_sym_pack(int32_t N, const int64_t* __restrict__ sptr, const int64_t* __restrict__ uptr,
@@ -341,12 +409,67 @@ int scan_exclusive(Ctx* c, const T* in, T* out, int64_t n) {
 
 }  // namespace
 
+// The coded indices, when the pattern allows them (else sym_coded stays false
+// and the products read the 4-byte columns and lower references).
+int build_sym_codes(Ctx* c) {
+  c->sym_coded = false;
+  dfree(&c->sym_ucode);
+  dfree(&c->sym_lcode);
+  const int64_t nwords = kOffRange / 32;
+  uint32_t* bits = nullptr;
+  int32_t* flags = nullptr;
+  UFC_TRY(dalloc(c, &bits, nwords));
+  UFC_TRY(dalloc(c, &flags, 1));
+  auto done = [&](int st) {
+    dfree(&bits);
+    dfree(&flags);
+    return st;
+  };
+  if (cudaMemsetAsync(bits, 0, sizeof(uint32_t) * nwords, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(flags, 0, sizeof(int32_t), c->stream) != cudaSuccess)
+    return done(cuda_fail(c, cudaGetLastError(), "symmetric codes"));
+  k_sym_offsets<<<grid_for(c->N, 256), 256, 0, c->stream>>>(c->N, c->nslices, c->uptr, c->ucol, bits, flags);
+  std::vector<uint32_t> h(nwords);
+  int32_t hf = 0;
+  if (cudaMemcpyAsync(h.data(), bits, sizeof(uint32_t) * nwords, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaMemcpyAsync(&hf, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return done(cuda_fail(c, cudaGetLastError(), "symmetric codes"));
+  if (hf) return done(UFC_STATUS_OK);  // not stencil-like, or rows too long
+  SymOffsets tab{};
+  int ntab = 0;
+  for (int64_t w = 0; w < nwords; ++w)
+    for (int b = 0; b < 32 && h[w] >> b; ++b)
+      if ((h[w] >> b) & 1u) {
+        if (ntab == kSymCodes) return done(UFC_STATUS_OK);  // too many distinct offsets
+        tab.off[ntab++] = (int32_t)(32 * w + b);
+      }
+  for (int q = ntab; q < 16; ++q) tab.off[q] = 0;
+  const int64_t rows = c->nslices * kSlice;
+  UFC_TRY(dalloc(c, &c->sym_ucode, rows * 16));
+  UFC_TRY(dalloc(c, &c->sym_lcode, rows * 16));
+  k_sym_codes<<<grid_for(rows, 256), 256, 0, c->stream>>>(c->N, c->nslices, c->uptr, c->lptr, c->ucol, c->lpos,
+                                                           c->lcol, c->s_ublocks, tab, ntab, c->sym_ucode,
+                                                           c->sym_lcode, flags);
+  if (cudaMemcpyAsync(&hf, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return done(cuda_fail(c, cudaGetLastError(), "symmetric codes"));
+  if (hf) {
+    dfree(&c->sym_ucode);
+    dfree(&c->sym_lcode);
+    return done(UFC_STATUS_OK);
+  }
+  c->sym_tab = tab;
+  c->sym_coded = true;
+  return done(UFC_STATUS_OK);
+}
+
 int build_pattern(Ctx* c) {
   if (c->E <= 0 || c->N <= 0) return fail(c, UFC_STATUS_INVALID, "ufc_pattern_build: mesh not set");
   release_graphs(c);
   dfree(&c->uptr); dfree(&c->ucol); dfree(&c->lptr); dfree(&c->lpos); dfree(&c->lcol); dfree(&c->s_lcnt);
-  dfree(&c->sval64); dfree(&c->sval32);
-  c->has_sym_pattern = c->has_sval64 = c->has_sval32 = false;
+  dfree(&c->sval64); dfree(&c->sval32); dfree(&c->sym_ucode); dfree(&c->sym_lcode);
+  c->has_sym_pattern = c->has_sval64 = c->has_sval32 = c->sym_coded = false;
   const int32_t N = c->N, E = c->E;
 
   // 1. colouring (host) and colour-grouped element lists
@@ -545,7 +668,7 @@ int build_sym_pattern(Ctx* c) {
   UFC_CUDA(c, cudaGetLastError());
   UFC_TRY(check_dev_err(c, "symmetric storage"));
   c->has_sym_pattern = true;
-  return UFC_STATUS_OK;
+  return build_sym_codes(c);
 }
 
 int pack_symmetric(Ctx* c, bool fp64, bool fp32) {

@@ -411,6 +411,111 @@ __global__ void __launch_bounds__(kSpmvBlock)
   }
 }
 
+// The symmetric product with coded indices (stencil-like patterns, see
+// build_sym_codes): each row loads its 16 upper and 16 lower code bytes with
+// two 16-byte loads when the warp starts, so the loop loads no indices at all.
+// Upper step j: column row + off[code], its x gathered at once.  Lower step j:
+// column row - off[code], and the block (col, row) at position
+// uptr[col / 32] + 32 rank + col % 32 of the upper storage (uptr from L1):
+// one dependent load (the slice start) instead of a streamed position and
+// column.  Same summation order as k_spmv_sym, so the same results bit for bit.
+template <typename TV, typename TX, typename TA, int MODE>
+__global__ void __launch_bounds__(kSpmvBlock)
+    k_spmv_symc(int32_t N, int64_t nrows_pad, const int64_t* __restrict__ uptr, const int64_t* __restrict__ lptr,
+                const uint4* __restrict__ ucode, const uint4* __restrict__ lcode, SymOffsets tab,
+                const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y,
+                CgScalars* __restrict__ scal, double* __restrict__ partials) {
+  pdl_enter();
+  if (MODE == kCg && halted(scal)) return;
+  __shared__ int32_t soff[16];
+  if (threadIdx.x < 16) soff[threadIdx.x] = tab.off[threadIdx.x];
+  __syncthreads();
+  const int64_t row = (int64_t)blockIdx.x * kSpmvBlock + threadIdx.x;
+  double dot[1] = {0.0};
+  if (row < nrows_pad) {
+    const int64_t s = row >> 5;
+    const int t = (int)(row & 31);
+    TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
+    const int64_t ub = uptr[s];
+    const int ulen = (int)((uptr[s + 1] - ub) >> 5);
+    const int llen = (int)((lptr[s + 1] - lptr[s]) >> 5);
+    const uint4 uc = __ldcs(ucode + row), lc = __ldcs(lcode + row);
+    uint64_t ulo = uc.x | ((uint64_t)uc.y << 32), uhi = uc.z | ((uint64_t)uc.w << 32);
+    uint64_t llo = lc.x | ((uint64_t)lc.y << 32), lhi = lc.z | ((uint64_t)lc.w << 32);
+    const TV* uvp = val + 9 * ub + t;
+    if (t == 0) {
+      const int k1 = (sizeof(TV) == 8 ? 4 : 8) < ulen ? (sizeof(TV) == 8 ? 4 : 8) : ulen;
+      if (k1 > 0)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(val + 9 * ub),
+                     "r"((unsigned)(k1 * 288 * (int)sizeof(TV)))
+                     : "memory");
+    }
+    auto upper = [&](int j) {
+      const unsigned code = (unsigned)(ulo & 0xFF);
+      ulo = (ulo >> 8) | (uhi << 56);
+      uhi >>= 8;
+      TA x0 = TA(0), x1 = TA(0), x2 = TA(0);
+      if (code != kSymCodes) {
+        const int64_t cj = row + soff[code];
+        x0 = (TA)__ldg(x + 3 * cj);
+        x1 = (TA)__ldg(x + 3 * cj + 1);
+        x2 = (TA)__ldg(x + 3 * cj + 2);
+      }
+      const TV* v = uvp + 288 * (int64_t)j;
+      a0 += (TA)v[0] * x0 + (TA)v[32] * x1 + (TA)v[64] * x2;
+      a1 += (TA)v[96] * x0 + (TA)v[128] * x1 + (TA)v[160] * x2;
+      a2 += (TA)v[192] * x0 + (TA)v[224] * x1 + (TA)v[256] * x2;
+    };
+    auto lower = [&](int) {
+      const unsigned b = (unsigned)(llo & 0xFF);
+      llo = (llo >> 8) | (lhi << 56);
+      lhi >>= 8;
+      if (b != 0xFFu) {
+        const int64_t cj = row - soff[b >> 4];
+        const int64_t P = __ldg(uptr + (cj >> 5)) + 32 * (int64_t)(b & 15u) + (cj & 31);
+        const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
+        const TV* v = val + 9 * (P & ~int64_t(31)) + (P & 31);
+        a0 += (TA)__ldg(v) * x0 + (TA)__ldg(v + 96) * x1 + (TA)__ldg(v + 192) * x2;
+        a1 += (TA)__ldg(v + 32) * x0 + (TA)__ldg(v + 128) * x1 + (TA)__ldg(v + 224) * x2;
+        a2 += (TA)__ldg(v + 64) * x0 + (TA)__ldg(v + 160) * x1 + (TA)__ldg(v + 256) * x2;
+      }
+    };
+    const int mlen = ulen < llen ? ulen : llen;
+    int j = 0;
+#pragma unroll 1
+    for (; j + 1 < mlen; j += 2) {
+      upper(j);
+      lower(j);
+      upper(j + 1);
+      lower(j + 1);
+    }
+    for (; j < mlen; ++j) {
+      upper(j);
+      lower(j);
+    }
+    for (int k = mlen; k < ulen; ++k) upper(k);
+    for (int k = mlen; k < llen; ++k) lower(k);
+    if (row < N) {
+      y[3 * row] = (TX)a0;
+      y[3 * row + 1] = (TX)a1;
+      y[3 * row + 2] = (TX)a2;
+      if (MODE == kCg)
+        dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
+    }
+  }
+  if (MODE == kCg) {
+    double tot[1];
+    if (grid_sum<1, sizeof(TV) == 4>(dot, partials, &scal->ticket[0], tot)) {
+      scal->pq = tot[0];
+      if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
+        scal->stop = 3;
+      } else {
+        scal->alpha = scal->rz / tot[0];
+      }
+    }
+  }
+}
+
 // The symmetric product with SPLIT warps per slice for meshes with too few
 // slices to fill the GPU one warp each: warp `part` of a slice takes the
 // upper and lower steps j = part, part + SPLIT, ..., and the row sums of the
@@ -706,8 +811,13 @@ template <typename TV, typename TX, typename TA, int MODE>
 void launch_spmv_sym(const Ctx* c, int grid, cudaStream_t st, const TV* val, const TX* x, TX* y) {
   switch (spmv_split(c)) {
     case 1:
-      launch_mode<MODE>(k_spmv_sym<TV, TX, TA, MODE>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice, c->uptr,
-                        c->ucol, c->lptr, c->lpos, c->lcol, val, x, y, c->scal, c->partials);
+      if (c->sym_coded)
+        launch_mode<MODE>(k_spmv_symc<TV, TX, TA, MODE>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice, c->uptr,
+                          c->lptr, reinterpret_cast<const uint4*>(c->sym_ucode),
+                          reinterpret_cast<const uint4*>(c->sym_lcode), c->sym_tab, val, x, y, c->scal, c->partials);
+      else
+        launch_mode<MODE>(k_spmv_sym<TV, TX, TA, MODE>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice, c->uptr,
+                          c->ucol, c->lptr, c->lpos, c->lcol, val, x, y, c->scal, c->partials);
       break;
     case 2: launch_spmv_sym_split<TV, TX, TA, MODE, 2>(c, st, val, x, y); break;
     case 4: launch_spmv_sym_split<TV, TX, TA, MODE, 4>(c, st, val, x, y); break;
@@ -1058,9 +1168,12 @@ int64_t spmv_bytes(const Ctx* c, int precision) {
   const int64_t sx = precision == UFC_PRECISION_FP32_REFINE ? 4 : 8;  // vector entry
   const bool sym = precision == UFC_PRECISION_FP64 ? c->has_sval64 : c->has_sval32;
   if (sym) {
+    const int64_t upper = (c->nnzb + c->N) / 2, lower = (c->nnzb - c->N) / 2;
+    // coded indices (one-warp-per-slice form): upper values, 32 code bytes per
+    // row, x and y; the lower values are re-read from L2
+    if (c->sym_coded && spmv_split(c) == 1) return upper * 9 * sv + 32 * c->nslices * kSlice + 2 * c->n * sx;
     // symmetric storage: upper blocks (values + column), lower references
     // (position + column; their values are re-read from L2), x and y
-    const int64_t upper = (c->nnzb + c->N) / 2, lower = (c->nnzb - c->N) / 2;
     return upper * (9 * sv + 4) + lower * 8 + 2 * c->n * sx;
   }
   return c->nnzb * (9 * sv + 4) + 4 * ((int64_t)c->N + 1) + 2 * c->n * sx;

@@ -60,6 +60,13 @@ enum DevErr : int32_t {
 
 struct Mg;  // multigrid hierarchy (mg.cu)
 
+// Block-column offsets (col - row) of the upper half of a stencil-like block
+// pattern: entry k of a row's coded index is the position of its offset here.
+constexpr int kSymCodes = 15;      // offsets a code can name; code 15 = no block
+struct SymOffsets {
+  int32_t off[16];
+};
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;  // own non-blocking stream: all work runs here
@@ -120,6 +127,15 @@ struct Ctx {
   double* sval64 = nullptr;              // [(s_ublocks + 32) * 9]
   float* sval32 = nullptr;
   bool has_sval64 = false, has_sval32 = false;
+  // coded indices of the symmetric storage (when every slice has at most 16
+  // upper and 16 lower steps and the pattern has at most 15 distinct upper
+  // offsets): per row 16 bytes of upper codes and 16 of lower codes, one
+  // 16-byte load each; a lower code holds the offset code (high nibble) and
+  // the rank of the block in its row's upper list (low nibble)
+  bool sym_coded = false;
+  SymOffsets sym_tab{};
+  uint8_t* sym_ucode = nullptr;          // [nslices * 32 * 16]
+  uint8_t* sym_lcode = nullptr;
 
   // Dirichlet set
   uint8_t* fixed = nullptr;  // [n]
@@ -173,6 +189,7 @@ int check_dev_err(Ctx* c, const char* where);
 // pattern.cu
 int build_pattern(Ctx* c);
 int build_sym_pattern(Ctx* c);
+int build_sym_codes(Ctx* c);
 int pack_symmetric(Ctx* c, bool fp64, bool fp32);  // full SELL values -> symmetric SpMV copies
 int export_csr(Ctx* c, const ufc_csr_export_arg* a);
 
