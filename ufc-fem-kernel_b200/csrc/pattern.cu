@@ -268,7 +268,8 @@ __global__ void k_sym_offsets(int32_t N, int64_t nslices, const int64_t* __restr
       atomicOr(flags, 1);
       continue;
     }
-    atomicOr(bits + (d >> 5), 1u << (d & 31));
+    const uint32_t m = 1u << (d & 31);
+    if (!(bits[d >> 5] & m)) atomicOr(bits + (d >> 5), m);  // most rows repeat the same few bits
   }
 }
 
