@@ -310,3 +310,46 @@ def test_symmetric_coded_indices_large_mesh(pkg, orc):
     nrows = (p.n_nodes + 31) // 32 * 32
     upper = (info.nnzb + p.n_nodes) // 2
     assert t["spmv_bytes"] == upper * 72 + 32 * nrows + 16 * p.n_dof
+
+
+def _renumbered(pkg, p, seed):
+    """The same problem with its nodes numbered in a random order: the block
+    pattern is then not stencil-like (many distinct offsets col - row), so the
+    products read 4-byte column indices instead of the coded ones."""
+    perm = np.random.default_rng(seed).permutation(p.n_nodes)  # new id of old node i
+    coords = np.empty_like(p.coords)
+    coords[perm] = p.coords
+    conn = perm[p.conn].astype(np.int32)
+    dof_map = (3 * perm[:, None] + np.arange(3)).ravel()  # old dof -> new dof
+    order = np.argsort(dof_map[p.fixed])
+    fixed = dof_map[p.fixed][order].astype(np.int32)
+    f = np.empty_like(p.f)
+    f[dof_map] = p.f
+    return pkg.mesh.Problem(p.name + "_renumbered", p.shape, coords, conn, p.mat_model_id, p.props, fixed,
+                            p.fixed_values[order], f), dof_map
+
+
+@pytest.mark.parametrize("shape", [(8, 4, 4), (64, 48, 48)])
+def test_unstructured_numbering_uses_plain_indices(pkg, orc, shape):
+    """Random node numbering: full and symmetric products and solves agree with
+    the oracle and with the structured numbering of the same mesh (coded
+    indices there, 4-byte indices here; 64x48x48 takes the one-warp-per-slice
+    kernels, 8x4x4 the split ones)."""
+    p = pkg.mesh.lognormal_cantilever(*shape, seed=4)
+    q, dof_map = _renumbered(pkg, p, seed=11)
+    K = orc.Model(q).assemble()
+    x = np.random.default_rng(2).standard_normal(q.n_dof)
+    y_o = K.matvec(x)
+    scale = np.abs(y_o).max()
+    u_ref = None
+    for build in (pkg.BUILD_FP64 | pkg.BUILD_FP32_ROUNDED, pkg.BUILD_FP64 | pkg.BUILD_FP32_ROUNDED | pkg.BUILD_SYMMETRIC):
+        m = _model(pkg, q, build)
+        assert np.abs(m.spmv(x) - y_o).max() <= 1e-13 * scale
+        u, st = m.solve(pkg.lifted_rhs(m, q.f), pkg.SolverAlgo(tolerance=1e-10))
+        assert st.converged
+        if u_ref is None:
+            s = _model(pkg, p, build)
+            us, _ = s.solve(pkg.lifted_rhs(s, p.f), pkg.SolverAlgo(tolerance=1e-10))
+            u_ref = np.empty_like(us)
+            u_ref[dof_map] = us  # structured solution in the renumbered order
+        assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) <= 1e-9

@@ -135,7 +135,7 @@ void free_all(Ctx* c) {
   dfree(&c->brow); dfree(&c->bcol); dfree(&c->slice_ptr); dfree(&c->sell_col); dfree(&c->slot); dfree(&c->dpos);
   dfree(&c->val64); dfree(&c->val32); dfree(&c->dinv64); dfree(&c->dinv32);
   dfree(&c->uptr); dfree(&c->ucol); dfree(&c->lptr); dfree(&c->lpos); dfree(&c->lcol); dfree(&c->s_lcnt);
-  dfree(&c->sval64); dfree(&c->sval32); dfree(&c->sym_ucode); dfree(&c->sym_lcode);
+  dfree(&c->sval64); dfree(&c->sval32); dfree(&c->sym_ucode); dfree(&c->sym_lcode); dfree(&c->full_code);
   c->has_sym_pattern = c->has_sval64 = c->has_sval32 = false;
   dfree(&c->fixed); dfree(&c->fix_dofs); dfree(&c->fix_vals);
   dfree(&c->x64); dfree(&c->r64); dfree(&c->p64); dfree(&c->q64); dfree(&c->b64); dfree(&c->y64);

@@ -316,6 +316,50 @@ __global__ void k_sym_codes(int32_t N, int64_t nslices, const int64_t* __restric
   }
 }
 
+// Coded indices of the full SELL storage: the offsets col - row of the real
+// blocks as bits over [-kOffRange, kOffRange), then 32 code bytes per row.
+__global__ void k_full_offsets(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr,
+                               const int32_t* __restrict__ col, uint32_t* __restrict__ bits,
+                               int32_t* __restrict__ flags) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
+  const int64_t s = r / kSlice, t = r % kSlice;
+  const int64_t b = sptr[s], len = (sptr[s + 1] - b) / kSlice;
+  if (len > 32) atomicOr(flags, 2);
+  for (int64_t k = 0; k < len; ++k) {
+    const int64_t d = (int64_t)col[b + k * kSlice + t] - r + kOffRange;
+    if (d < 0 || d >= 2 * kOffRange) {
+      atomicOr(flags, 1);
+      continue;
+    }
+    const uint32_t m = 1u << (d & 31);
+    if (!(bits[d >> 5] & m)) atomicOr(bits + (d >> 5), m);
+  }
+}
+
+// Code of block k of row r at code[32 r + k]: index of col - row in tab, 255
+// for no block (k beyond the slice, or a row past the mesh).  Padding blocks of
+// a real row point at the row itself (offset 0) with zero values.
+__global__ void k_full_codes(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr,
+                             const int32_t* __restrict__ col, FullOffsets tab, int ntab, uint8_t* __restrict__ code,
+                             int32_t* __restrict__ flags) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nslices * kSlice) return;
+  const int64_t s = r / kSlice, t = r % kSlice;
+  const int64_t b = sptr[s], len = (sptr[s + 1] - b) / kSlice;
+  for (int k = 0; k < 32; ++k) {
+    uint8_t u = 255;
+    if (r < N && k < len) {
+      const int64_t d = (int64_t)col[b + k * kSlice + t] - r;
+      int q = 0;
+      while (q < ntab && tab.off[q] != d) ++q;
+      if (q == ntab) atomicOr(flags, 4);
+      else u = (uint8_t)q;
+    }
+    code[r * 32 + k] = u;
+  }
+}
+
 // Copy the upper blocks of the full SELL values into the symmetric storage.
 template <typename TO>
 __global__ void k_sym_pack(int32_t N, const int64_t* __restrict__ sptr, const int64_t* __restrict__ uptr,
@@ -465,11 +509,63 @@ int build_sym_codes(Ctx* c) {
   return done(UFC_STATUS_OK);
 }
 
+// The coded indices of the full storage, when the pattern allows them (else
+// full_coded stays false and the products read the 4-byte columns).
+int build_full_codes(Ctx* c) {
+  c->full_coded = false;
+  dfree(&c->full_code);
+  const int64_t nwords = 2 * kOffRange / 32;
+  uint32_t* bits = nullptr;
+  int32_t* flags = nullptr;
+  UFC_TRY(dalloc(c, &bits, nwords));
+  UFC_TRY(dalloc(c, &flags, 1));
+  auto done = [&](int st) {
+    dfree(&bits);
+    dfree(&flags);
+    return st;
+  };
+  if (cudaMemsetAsync(bits, 0, sizeof(uint32_t) * nwords, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(flags, 0, sizeof(int32_t), c->stream) != cudaSuccess)
+    return done(cuda_fail(c, cudaGetLastError(), "full codes"));
+  k_full_offsets<<<grid_for(c->N, 256), 256, 0, c->stream>>>(c->N, c->nslices, c->slice_ptr, c->sell_col, bits,
+                                                             flags);
+  std::vector<uint32_t> h(nwords);
+  int32_t hf = 0;
+  if (cudaMemcpyAsync(h.data(), bits, sizeof(uint32_t) * nwords, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaMemcpyAsync(&hf, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return done(cuda_fail(c, cudaGetLastError(), "full codes"));
+  if (hf) return done(UFC_STATUS_OK);
+  FullOffsets tab{};
+  int ntab = 0;
+  for (int64_t w = 0; w < nwords; ++w)
+    for (int b = 0; b < 32 && h[w] >> b; ++b)
+      if ((h[w] >> b) & 1u) {
+        if (ntab == kFullCodes) return done(UFC_STATUS_OK);
+        tab.off[ntab++] = (int32_t)(32 * w + b - kOffRange);
+      }
+  const int64_t rows = c->nslices * kSlice;
+  UFC_TRY(dalloc(c, &c->full_code, rows * 32));
+  k_full_codes<<<grid_for(rows, 256), 256, 0, c->stream>>>(c->N, c->nslices, c->slice_ptr, c->sell_col, tab, ntab,
+                                                           c->full_code, flags);
+  if (cudaMemcpyAsync(&hf, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return done(cuda_fail(c, cudaGetLastError(), "full codes"));
+  if (hf) {
+    dfree(&c->full_code);
+    return done(UFC_STATUS_OK);
+  }
+  c->full_tab = tab;
+  c->full_coded = true;
+  return done(UFC_STATUS_OK);
+}
+
 int build_pattern(Ctx* c) {
   if (c->E <= 0 || c->N <= 0) return fail(c, UFC_STATUS_INVALID, "ufc_pattern_build: mesh not set");
   release_graphs(c);
   dfree(&c->uptr); dfree(&c->ucol); dfree(&c->lptr); dfree(&c->lpos); dfree(&c->lcol); dfree(&c->s_lcnt);
-  dfree(&c->sval64); dfree(&c->sval32); dfree(&c->sym_ucode); dfree(&c->sym_lcode);
+  dfree(&c->sval64); dfree(&c->sval32); dfree(&c->sym_ucode); dfree(&c->sym_lcode); dfree(&c->full_code);
+  c->full_coded = false;
   c->has_sym_pattern = c->has_sval64 = c->has_sval32 = c->sym_coded = false;
   const int32_t N = c->N, E = c->E;
 
@@ -573,7 +669,7 @@ int build_pattern(Ctx* c) {
   dfree(&c->val32);
   c->has_val64 = c->has_val32 = false;
   c->has_pattern = true;
-  return UFC_STATUS_OK;
+  return build_full_codes(c);
 }
 
 int export_csr(Ctx* c, const ufc_csr_export_arg* a) {

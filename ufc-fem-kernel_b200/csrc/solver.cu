@@ -234,6 +234,109 @@ __global__ void __launch_bounds__(kSpmvBlock)
   }
 }
 
+// 32 code bytes of one row, consumed from the front one block step at a time.
+struct Code256 {
+  uint64_t w0, w1, w2, w3;
+  __device__ __forceinline__ unsigned front() const { return (unsigned)(w0 & 0xFFu); }
+  template <int B>
+  __device__ __forceinline__ void drop() {
+    if constexpr (B >= 8) {
+      w0 = w1;
+      w1 = w2;
+      w2 = w3;
+      w3 = 0;
+    } else {
+      constexpr int sh = 8 * B;
+      w0 = (w0 >> sh) | (w1 << (64 - sh));
+      w1 = (w1 >> sh) | (w2 << (64 - sh));
+      w2 = (w2 >> sh) | (w3 << (64 - sh));
+      w3 >>= sh;
+    }
+  }
+};
+
+// y = K x on the full SELL storage with coded indices (see build_full_codes):
+// each row loads its 32 code bytes with two 16-byte loads when the warp
+// starts, and block j's column is row + off[code j], so no column index is
+// loaded inside the loop.  SPLIT warps per slice on small meshes, as
+// k_spmv_split (SPLIT = 1: one warp per slice, as k_spmv), with the same
+// summation order, so the same results bit for bit.
+template <typename TV, typename TX, typename TA, int MODE, int SPLIT>
+__global__ void __launch_bounds__(kSpmvBlock)
+    k_spmvc(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const uint4* __restrict__ code,
+            FullOffsets tab, const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y,
+            CgScalars* __restrict__ scal, double* __restrict__ partials) {
+  pdl_enter();
+  if (MODE == kCg && halted(scal)) return;
+  __shared__ int32_t soff[32];
+  if (threadIdx.x < 32) soff[threadIdx.x] = tab.off[threadIdx.x];
+  __syncthreads();
+  constexpr int kWarps = kSpmvBlock / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int part = warp % SPLIT;
+  const int64_t s = (int64_t)blockIdx.x * (kWarps / SPLIT) + warp / SPLIT;
+  const int64_t row = s * kSlice + lane;
+  TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
+  if (s < nslices) {
+    const int64_t base = sptr[s];
+    const int len = (int)((sptr[s + 1] - base) >> 5);
+    const uint4 c0 = __ldcs(code + 2 * row), c1 = __ldcs(code + 2 * row + 1);
+    Code256 cw{c0.x | ((uint64_t)c0.y << 32), c0.z | ((uint64_t)c0.w << 32), c1.x | ((uint64_t)c1.y << 32),
+               c1.z | ((uint64_t)c1.w << 32)};
+    for (int q = 0; q < part; ++q) cw.template drop<1>();
+    const TV* vp = val + 9 * base + lane;
+#pragma unroll 2
+    for (int j = part; j < len; j += SPLIT) {
+      const unsigned cd = cw.front();
+      cw.template drop<SPLIT>();
+      TA x0 = TA(0), x1 = TA(0), x2 = TA(0);
+      if (cd != 255u) {
+        const int64_t cj = row + soff[cd];
+        x0 = (TA)__ldg(x + 3 * cj);
+        x1 = (TA)__ldg(x + 3 * cj + 1);
+        x2 = (TA)__ldg(x + 3 * cj + 2);
+      }
+      const TV* v = vp + 288 * (int64_t)j;
+      a0 += (TA)__ldcs(v) * x0 + (TA)__ldcs(v + 32) * x1 + (TA)__ldcs(v + 64) * x2;
+      a1 += (TA)__ldcs(v + 96) * x0 + (TA)__ldcs(v + 128) * x1 + (TA)__ldcs(v + 160) * x2;
+      a2 += (TA)__ldcs(v + 192) * x0 + (TA)__ldcs(v + 224) * x1 + (TA)__ldcs(v + 256) * x2;
+    }
+  }
+  if constexpr (SPLIT > 1) {
+    __shared__ TA sh[kWarps][3][32];
+    sh[warp][0][lane] = a0;
+    sh[warp][1][lane] = a1;
+    sh[warp][2][lane] = a2;
+    __syncthreads();
+    if (part == 0) {
+#pragma unroll
+      for (int q = 1; q < SPLIT; ++q) {
+        a0 += sh[warp + q][0][lane];
+        a1 += sh[warp + q][1][lane];
+        a2 += sh[warp + q][2][lane];
+      }
+    }
+  }
+  double dot[1] = {0.0};
+  if (part == 0 && s < nslices && row < N) {
+    y[3 * row] = (TX)a0;
+    y[3 * row + 1] = (TX)a1;
+    y[3 * row + 2] = (TX)a2;
+    if (MODE == kCg) dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
+  }
+  if (MODE == kCg) {
+    double tot[1];
+    if (grid_sum<1>(dot, partials, &scal->ticket[0], tot)) {
+      scal->pq = tot[0];
+      if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
+        scal->stop = 3;
+      } else {
+        scal->alpha = scal->rz / tot[0];
+      }
+    }
+  }
+}
+
 // Warps per SELL slice: the smallest power of two (<= 8) that puts at least
 // 32 warps per SM in flight.
 int spmv_split(const Ctx* c) {
@@ -250,6 +353,13 @@ int spmv_split(const Ctx* c) {
 
 template <typename TV, typename TX, typename TA, int MODE, bool DIFF, int SPLIT>
 void launch_spmv_split(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
+  if (!DIFF && c->full_coded) {
+    constexpr int per_block = kSpmvBlock / 32 / SPLIT;
+    const int grid = (int)((c->nslices + per_block - 1) / per_block);
+    launch_mode<MODE>(k_spmvc<TV, TX, TA, MODE, SPLIT>, grid, kSpmvBlock, st, c->N, c->nslices, c->slice_ptr,
+                      reinterpret_cast<const uint4*>(c->full_code), c->full_tab, val, x, y, c->scal, c->partials);
+    return;
+  }
   if constexpr (SPLIT == 1) {
     const int grid = (int)((c->nslices * kSlice + kSpmvBlock - 1) / kSpmvBlock);
     launch_mode<MODE>(k_spmv<TV, TX, TA, MODE, DIFF>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice,
@@ -1176,6 +1286,8 @@ int64_t spmv_bytes(const Ctx* c, int precision) {
     // (position + column; their values are re-read from L2), x and y
     return upper * (9 * sv + 4) + lower * 8 + 2 * c->n * sx;
   }
+  // coded indices: values, 32 code bytes per row, x and y
+  if (c->full_coded && !(sv == 4 && c->val32_diff)) return c->nnzb * 9 * sv + 32 * c->nslices * kSlice + 2 * c->n * sx;
   return c->nnzb * (9 * sv + 4) + 4 * ((int64_t)c->N + 1) + 2 * c->n * sx;
 }
 

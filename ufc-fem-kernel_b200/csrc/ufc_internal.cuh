@@ -66,6 +66,12 @@ constexpr int kSymCodes = 15;      // offsets a code can name; code 15 = no bloc
 struct SymOffsets {
   int32_t off[16];
 };
+// The same for the full block pattern (col - row of either sign): up to 31
+// offsets, code 255 = no block; 32 code bytes per row.
+constexpr int kFullCodes = 31;
+struct FullOffsets {
+  int32_t off[32];
+};
 
 struct Ctx {
   int device = 0;
@@ -133,6 +139,11 @@ struct Ctx {
   // 16-byte load each; a lower code holds the offset code (high nibble) and
   // the rank of the block in its row's upper list (low nibble)
   bool sym_coded = false;
+  // coded indices of the full SELL storage (rows of at most 32 blocks, at most
+  // 31 distinct offsets): 32 code bytes per row, lane-major
+  bool full_coded = false;
+  FullOffsets full_tab{};
+  uint8_t* full_code = nullptr;          // [nslices * 32 * 32]
   SymOffsets sym_tab{};
   uint8_t* sym_ucode = nullptr;          // [nslices * 32 * 16]
   uint8_t* sym_lcode = nullptr;
@@ -190,6 +201,7 @@ int check_dev_err(Ctx* c, const char* where);
 int build_pattern(Ctx* c);
 int build_sym_pattern(Ctx* c);
 int build_sym_codes(Ctx* c);
+int build_full_codes(Ctx* c);
 int pack_symmetric(Ctx* c, bool fp64, bool fp32);  // full SELL values -> symmetric SpMV copies
 int export_csr(Ctx* c, const ufc_csr_export_arg* a);
 
