@@ -85,10 +85,6 @@ int vec_grid(int64_t n) {
 
 enum SpmvMode { kPlain = 0, kCg = 1 };
 
-// The coded symmetric product with one warp for the upper and one for the lower
-// blocks of each slice (k_spmv_symc_roles) instead of one warp doing both.
-constexpr bool kSymRoles = true;
-
 // The kernels of a CG iteration do nothing once the run has stopped or asked
 // for an FP64 residual replacement: a batch of iterations launched as one graph
 // then idles from the triggering iteration on, so the replacement happens at
@@ -357,11 +353,12 @@ int spmv_split(const Ctx* c) {
 
 template <typename TV, typename TX, typename TA, int MODE, bool DIFF, int SPLIT>
 void launch_spmv_split(const Ctx* c, cudaStream_t st, const TV* val, const TX* x, TX* y) {
-  // coded indices with one warp per slice only: with SPLIT warps per slice each
-  // warp would load the row's 32 code bytes, more than its share of 4-byte
-  // columns (measured on the 64x32x32 J2 bar: 53.7 against 51.8 us per CG
+  // coded indices with FP32 values and one warp per slice only (measured on
+  // B200: 192x96x96 FP32 product 297 against 325 us, FP64 582 against 568 us;
+  // with SPLIT warps per slice each warp loads the row's 32 code bytes, more
+  // than its share of 4-byte columns: J2 bar 53.7 against 51.8 us per CG
   // iteration)
-  if (!DIFF && SPLIT == 1 && c->full_coded) {
+  if (!DIFF && SPLIT == 1 && sizeof(TV) == 4 && c->full_coded) {
     constexpr int per_block = kSpmvBlock / 32 / SPLIT;
     const int grid = (int)((c->nslices + per_block - 1) / per_block);
     launch_mode<MODE>(k_spmvc<TV, TX, TA, MODE, SPLIT>, grid, kSpmvBlock, st, c->N, c->nslices, c->slice_ptr,
@@ -620,98 +617,6 @@ __global__ void __launch_bounds__(kSpmvBlock)
       if (MODE == kCg)
         dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
     }
-  }
-  if (MODE == kCg) {
-    double tot[1];
-    if (grid_sum<1, sizeof(TV) == 4>(dot, partials, &scal->ticket[0], tot)) {
-      scal->pq = tot[0];
-      if (!(fabs(tot[0]) > 1e-300) || !isfinite(tot[0])) {
-        scal->stop = 3;
-      } else {
-        scal->alpha = scal->rz / tot[0];
-      }
-    }
-  }
-}
-
-// The coded symmetric product with two warps per slice by kind of block: the
-// even warp streams the slice's upper blocks (independent loads only), the odd
-// warp gathers its lower blocks (slice start from L1, values from L2); their
-// row sums are added in shared memory, upper first, then written.
-template <typename TV, typename TX, typename TA, int MODE>
-__global__ void __launch_bounds__(kSpmvBlock)
-    k_spmv_symc_roles(int32_t N, int64_t nslices, const int64_t* __restrict__ uptr, const int64_t* __restrict__ lptr,
-                      const uint4* __restrict__ ucode, const uint4* __restrict__ lcode, SymOffsets tab,
-                      const TV* __restrict__ val, const TX* __restrict__ x, TX* __restrict__ y,
-                      CgScalars* __restrict__ scal, double* __restrict__ partials) {
-  pdl_enter();
-  if (MODE == kCg && halted(scal)) return;
-  __shared__ int32_t soff[16];
-  __shared__ TA sh[kSpmvBlock / 32][3][32];
-  if (threadIdx.x < 16) soff[threadIdx.x] = tab.off[threadIdx.x];
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, role = warp & 1;
-  const int64_t s = (int64_t)blockIdx.x * (kSpmvBlock / 64) + (warp >> 1);
-  const int64_t row = s * kSlice + lane;
-  TA a0 = TA(0), a1 = TA(0), a2 = TA(0);
-  if (s < nslices) {
-    if (role == 0) {
-      const int64_t ub = uptr[s];
-      const int ulen = (int)((uptr[s + 1] - ub) >> 5);
-      const uint4 uc = __ldcs(ucode + row);
-      uint64_t lo = uc.x | ((uint64_t)uc.y << 32), hi = uc.z | ((uint64_t)uc.w << 32);
-      const TV* uvp = val + 9 * ub + lane;
-#pragma unroll 2
-      for (int j = 0; j < ulen; ++j) {
-        const unsigned code = (unsigned)(lo & 0xFF);
-        lo = (lo >> 8) | (hi << 56);
-        hi >>= 8;
-        TA x0 = TA(0), x1 = TA(0), x2 = TA(0);
-        if (code != kSymCodes) {
-          const int64_t cj = row + soff[code];
-          x0 = (TA)__ldg(x + 3 * cj);
-          x1 = (TA)__ldg(x + 3 * cj + 1);
-          x2 = (TA)__ldg(x + 3 * cj + 2);
-        }
-        const TV* v = uvp + 288 * (int64_t)j;
-        a0 += (TA)v[0] * x0 + (TA)v[32] * x1 + (TA)v[64] * x2;
-        a1 += (TA)v[96] * x0 + (TA)v[128] * x1 + (TA)v[160] * x2;
-        a2 += (TA)v[192] * x0 + (TA)v[224] * x1 + (TA)v[256] * x2;
-      }
-    } else {
-      const int llen = (int)((lptr[s + 1] - lptr[s]) >> 5);
-      const uint4 lc = __ldcs(lcode + row);
-      uint64_t lo = lc.x | ((uint64_t)lc.y << 32), hi = lc.z | ((uint64_t)lc.w << 32);
-#pragma unroll 2
-      for (int j = 0; j < llen; ++j) {
-        const unsigned b = (unsigned)(lo & 0xFF);
-        lo = (lo >> 8) | (hi << 56);
-        hi >>= 8;
-        if (b != 0xFFu) {
-          const int64_t cj = row - soff[b >> 4];
-          const int64_t P = __ldg(uptr + (cj >> 5)) + 32 * (int64_t)(b & 15u) + (cj & 31);
-          const TA x0 = (TA)__ldg(x + 3 * cj), x1 = (TA)__ldg(x + 3 * cj + 1), x2 = (TA)__ldg(x + 3 * cj + 2);
-          const TV* v = val + 9 * (P & ~int64_t(31)) + (P & 31);
-          a0 += (TA)__ldg(v) * x0 + (TA)__ldg(v + 96) * x1 + (TA)__ldg(v + 192) * x2;
-          a1 += (TA)__ldg(v + 32) * x0 + (TA)__ldg(v + 128) * x1 + (TA)__ldg(v + 224) * x2;
-          a2 += (TA)__ldg(v + 64) * x0 + (TA)__ldg(v + 160) * x1 + (TA)__ldg(v + 256) * x2;
-        }
-      }
-    }
-  }
-  sh[warp][0][lane] = a0;
-  sh[warp][1][lane] = a1;
-  sh[warp][2][lane] = a2;
-  __syncthreads();
-  double dot[1] = {0.0};
-  if (role == 0 && s < nslices && row < N) {
-    a0 += sh[warp + 1][0][lane];
-    a1 += sh[warp + 1][1][lane];
-    a2 += sh[warp + 1][2][lane];
-    y[3 * row] = (TX)a0;
-    y[3 * row + 1] = (TX)a1;
-    y[3 * row + 2] = (TX)a2;
-    if (MODE == kCg) dot[0] = (double)((TA)x[3 * row] * a0 + (TA)x[3 * row + 1] * a1 + (TA)x[3 * row + 2] * a2);
   }
   if (MODE == kCg) {
     double tot[1];
@@ -1021,11 +926,7 @@ template <typename TV, typename TX, typename TA, int MODE>
 void launch_spmv_sym(const Ctx* c, int grid, cudaStream_t st, const TV* val, const TX* x, TX* y) {
   switch (spmv_split(c)) {
     case 1:
-      if (c->sym_coded && kSymRoles)
-        launch_mode<MODE>(k_spmv_symc_roles<TV, TX, TA, MODE>, (int)((c->nslices + 3) / 4), kSpmvBlock, st, c->N,
-                          c->nslices, c->uptr, c->lptr, reinterpret_cast<const uint4*>(c->sym_ucode),
-                          reinterpret_cast<const uint4*>(c->sym_lcode), c->sym_tab, val, x, y, c->scal, c->partials);
-      else if (c->sym_coded)
+      if (c->sym_coded)
         launch_mode<MODE>(k_spmv_symc<TV, TX, TA, MODE>, grid, kSpmvBlock, st, c->N, c->nslices * kSlice, c->uptr,
                           c->lptr, reinterpret_cast<const uint4*>(c->sym_ucode),
                           reinterpret_cast<const uint4*>(c->sym_lcode), c->sym_tab, val, x, y, c->scal, c->partials);
@@ -1391,7 +1292,7 @@ int64_t spmv_bytes(const Ctx* c, int precision) {
     return upper * (9 * sv + 4) + lower * 8 + 2 * c->n * sx;
   }
   // coded indices: values, 32 code bytes per row, x and y
-  if (c->full_coded && !(sv == 4 && c->val32_diff) && spmv_split(c) == 1)
+  if (c->full_coded && sv == 4 && !c->val32_diff && spmv_split(c) == 1)
     return c->nnzb * 9 * sv + 32 * c->nslices * kSlice + 2 * c->n * sx;
   return c->nnzb * (9 * sv + 4) + 4 * ((int64_t)c->N + 1) + 2 * c->n * sx;
 }
