@@ -1002,13 +1002,17 @@ int get_graph(const Run& R, const Vecs<TV, TX>& V, int batch, cudaGraphExec_t* o
   // one cached graph per (value, vector, accumulator) type combination
   const int slot = sizeof(TV) == 8 ? 0 : sizeof(TX) == 8 ? 3 : sizeof(TA) == 8 ? 2 : 1;
   // graphs are rebuilt when a buffer they read, the preconditioner, the storage
-  // (symmetric or full) or the FP32 SpMV form (difference or plain) changes; a
-  // reassembly into the same arrays keeps them
+  // (symmetric or full), the SpMV form (FP32 difference form, coded indices)
+  // or the sizes baked into their launches (DOFs, slices) change; a reassembly
+  // into the same arrays keeps them.  The vector and pattern buffers are not in
+  // the key: ensure_vectors, build_sym_pattern and pack_symmetric, which
+  // reallocate them, release the graphs themselves.
   const void* key = (const void*)V.dinv;
   const void* val = (const void*)V.val;
-  const int form = (V.sym ? 1 : 0) | (c->val32_diff ? 2 : 0);
+  const int form = (V.sym ? 1 : 0) | (c->val32_diff ? 2 : 0) | (c->sym_coded ? 4 : 0) | (c->full_coded ? 8 : 0);
   if (c->cg_graph[slot] && c->cg_graph_batch[slot] == batch && c->cg_graph_key[slot] == key &&
-      c->cg_graph_val[slot] == val && c->cg_graph_form[slot] == form) {
+      c->cg_graph_val[slot] == val && c->cg_graph_form[slot] == form && c->cg_graph_n[slot] == R.n &&
+      c->cg_graph_slices[slot] == c->nslices) {
     *out = c->cg_graph[slot];
     return UFC_STATUS_OK;
   }
@@ -1028,6 +1032,8 @@ int get_graph(const Run& R, const Vecs<TV, TX>& V, int batch, cudaGraphExec_t* o
   c->cg_graph_key[slot] = key;
   c->cg_graph_val[slot] = val;
   c->cg_graph_form[slot] = form;
+  c->cg_graph_n[slot] = R.n;
+  c->cg_graph_slices[slot] = c->nslices;
   *out = c->cg_graph[slot];
   return UFC_STATUS_OK;
 }
@@ -1273,6 +1279,7 @@ void release_graphs(Ctx* c) {
     c->cg_graph_key[k] = nullptr;
     c->cg_graph_val[k] = nullptr;
     c->cg_graph_form[k] = 0;
+    c->cg_graph_n[k] = c->cg_graph_slices[k] = 0;
   }
 }
 

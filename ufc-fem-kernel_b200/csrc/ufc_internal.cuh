@@ -189,6 +189,7 @@ struct Ctx {
   const void* cg_graph_val[kGraphSlots] = {};
   const void* cg_graph_key[kGraphSlots] = {};
   int cg_graph_form[kGraphSlots] = {};
+  int64_t cg_graph_n[kGraphSlots] = {}, cg_graph_slices[kGraphSlots] = {};
   std::vector<cudaEvent_t> ev_pool;
 };
 
