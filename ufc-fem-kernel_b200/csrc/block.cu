@@ -13,7 +13,9 @@
 // a row share them) and the row sums stay in registers.  With 4 to 32
 // right-hand sides the product (k_bspmv_pipe) streams each warp task's values,
 // columns and x lines through a shared-memory ring with cp.async, so that the
-// waits for memory hold no registers.  The vector kernels
+// waits for memory hold no registers.  With 16 right-hand sides on a
+// stencil-like pattern (coded full storage) k_bspmv_tile takes each half
+// slice's x nodes into shared memory once, by bulk copies, instead.  The vector kernels
 // give every thread the same G right-hand sides of successive dofs.
 // Each right-hand side has its own alpha, beta and stop test; a converged
 // right-hand side is frozen (alpha = beta = 0) while the others continue.
@@ -91,12 +93,13 @@ __device__ __forceinline__ void st_g(double* p, const double (&o)[G]) {
 // the same t % tpr are combined by shuffles, then the warps of the block in
 // order, then the blocks in order by the last block to finish.  Returns true
 // in the threads k < nr of that block, out[q] being the total of value q for
-// rhs k; the ticket is reset for the next launch.
-template <int G, int NV>
+// rhs k; the ticket is reset for the next launch.  BLK = threads per block.
+template <int G, int NV, int BLK = kBlk>
 __device__ bool rhs_grid_sum(double (&v)[NV][G], int tpr, int nr, double* __restrict__ partials, uint32_t* ticket,
                              double (&out)[NV]) {
-  __shared__ double sh[kWarps][NV][kMaxRhs];
-  __shared__ double fin[kBlk * NV];
+  constexpr int W = BLK / 32;
+  __shared__ double sh[W][NV][kMaxRhs];
+  __shared__ double fin[BLK * NV];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int o = 16; o >= tpr; o >>= 1)
@@ -114,7 +117,7 @@ __device__ bool rhs_grid_sum(double (&v)[NV][G], int tpr, int nr, double* __rest
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       double s = 0.0;
-      for (int ww = 0; ww < kWarps; ++ww) s += sh[ww][q][threadIdx.x];
+      for (int ww = 0; ww < W; ++ww) s += sh[ww][q][threadIdx.x];
       partials[((int64_t)blockIdx.x * NV + q) * kMaxRhs + threadIdx.x] = s;
     }
   }
@@ -125,7 +128,7 @@ __device__ bool rhs_grid_sum(double (&v)[NV][G], int tpr, int nr, double* __rest
   if (!last) return false;
   __threadfence();
   // last block: thread t sums the blocks b = t/nr (mod blockDim/nr) for rhs t % nr
-  const int k = threadIdx.x % nr, gi = threadIdx.x / nr, groups = kBlk / nr;
+  const int k = threadIdx.x % nr, gi = threadIdx.x / nr, groups = BLK / nr;
   double acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) acc[q] = 0.0;
@@ -378,6 +381,243 @@ __global__ void __launch_bounds__(kBlk, 3)
   }
 }
 
+// The x tile of a half slice (16 block rows) for the coded full storage: the
+// union of the column ranges [row0 + off_k, row0 + off_k + 16) over the
+// pattern's offsets, merged into nrange runs of nodes (run m starts at node
+// row0 + a[m], has len[m] nodes and sits at node sb[m] of the shared-memory
+// tile); node0[k] is the tile node of column row0 + off_k.  On a structured
+// mesh the 27 offsets give 9 runs of 18 nodes, so each x line of a tile is
+// read once instead of about 2.7 times.
+constexpr int kTileRows = 16;
+constexpr int kTileNr = 16;                        // right-hand sides (interleaved)
+constexpr int kTileCons = kTileRows * kTileNr / 2;  // consumer threads: 2 rhs of one row each
+constexpr int kTileBlk = kTileCons + 32;           // and one producer warp
+constexpr int kTileNodeBytes = 3 * kTileNr * 8;
+constexpr int kTileMaxNodes = 176;
+constexpr int kValPad = 10;                        // doubles per block in the tile value layout
+constexpr int kStageCodes = kTileRows * 32;        // code bytes of a tile
+constexpr int kStageVals = 32 * kTileRows * kValPad * 8;  // values of up to 32 steps
+struct BTile {
+  int32_t nrange, nodes;
+  int32_t a[kFullCodes + 1], len[kFullCodes + 1], sb[kFullCodes + 1], node0[kFullCodes + 1];
+};
+
+constexpr size_t tile_stage_bytes(int nodes) {
+  return (size_t)kStageCodes + kStageVals + (size_t)nodes * kTileNodeBytes;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Bounded wait for the completion of phase `parity` of an mbarrier; false when
+// it gave up (the caller records kDevTimeout).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (int it = 0; it < (1 << 20); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// The values of the full storage in tile order: half slice h of slice s holds
+// its len steps x 16 rows x kValPad doubles (the 9 of the block, row-major by
+// output component, then a zero) at 10 * sptr[s] + h * 160 * len, so that a
+// tile's values are one contiguous bulk copy and a row's block is five
+// 16-byte loads.
+__global__ void k_tile_vals(int64_t rows, const int64_t* __restrict__ sptr, const double* __restrict__ val,
+                            double* __restrict__ tv) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const int64_t sl = r >> 5;
+  const int t = (int)(r & 31);
+  const int64_t base = sptr[sl];
+  const int len = (int)((sptr[sl + 1] - base) >> 5);
+  double* o = tv + kValPad * base + (int64_t)(t >> 4) * (16 * kValPad) * len + (t & 15) * kValPad;
+  for (int j = 0; j < len; ++j) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) o[(int64_t)j * 16 * kValPad + c] = val[9 * (base + 32 * (int64_t)j) + 32 * c + t];
+    o[(int64_t)j * 16 * kValPad + 9] = 0.0;
+  }
+}
+
+// The codes in tile form: byte j of row r names the tile node of its column,
+// node0[code] + r % 16 (< kTileMaxNodes), or 255 past the row's slice length
+// and for rows past the mesh.
+__global__ void k_tile_codes(int64_t rows, const uint8_t* __restrict__ code, const BTile T,
+                             uint8_t* __restrict__ tc) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= rows * 32) return;
+  const unsigned cd = code[e];
+  tc[e] = cd == 255u ? (uint8_t)255 : (uint8_t)(T.node0[cd] + (int)((e >> 5) & 15));
+}
+
+// y = K x for 16 interleaved vectors from the coded full storage, one half
+// slice (16 rows) per tile, the blocks resident and looping over the tiles.
+// A producer warp moves each tile into one of two shared-memory stages with
+// bulk copies (cp.async.bulk on an mbarrier counting bytes): the 16 rows'
+// code bytes (tile form, k_tile_codes), their values (tile order,
+// k_tile_vals) and the runs of x nodes the codes name (384 contiguous bytes
+// per node), so that every x line of a tile crosses L2 once.  The 128
+// consumer threads (8 per row, 2 rhs each) multiply from shared memory while
+// the next tile lands, then release the stage; a step costs them one byte
+// extract, one address and eight 16-byte shared loads besides the 18 FMAs.  The same products in the same order as k_bspmv_pipe, so the same y.
+// Every wait is bounded; a wait that gives up sets kDevTimeout.
+template <int MODE>
+__global__ void __launch_bounds__(kTileBlk, 1)
+    k_bspmv_tile(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const uint8_t* __restrict__ tcode,
+                 const double* __restrict__ tv, const BTile T, const double* __restrict__ x,
+                 double* __restrict__ y, BScalars* __restrict__ s, double* __restrict__ partials,
+                 int32_t* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t full[2], empty[2];
+  if (MODE == 1 && s->stop) return;
+  const size_t stage_bytes = tile_stage_bytes(T.nodes);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&empty[q])), "r"(kTileCons / 32)
+                   : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int64_t tiles = nslices * 2;
+  bool late = false;
+  double dot[1][2] = {{0.0, 0.0}};
+  if (warp == kTileCons / 32) {
+    // producer: one lane issues the copies of the block's tiles in order
+    if (lane == 0) {
+      int k = 0;
+      for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+        const int st = k & 1;
+        if (k >= 2 && !mbar_wait(&empty[st], (uint32_t)((k >> 1) - 1) & 1u)) late = true;
+        unsigned char* sb = tsm + st * stage_bytes;
+        const int64_t sl = tile >> 1;
+        const int h = (int)(tile & 1);
+        const int64_t r0 = sl * kSlice + h * kTileRows;
+        const int64_t base = sptr[sl];
+        const int len = (int)((sptr[sl + 1] - base) >> 5);
+        const uint32_t vbytes = (uint32_t)len * (16 * kValPad * 8);
+        uint32_t bytes = kStageCodes + vbytes;
+        for (int m = 0; m < T.nrange; ++m) {
+          const int64_t lo = max(r0 + T.a[m], (int64_t)0), hi = min(r0 + T.a[m] + T.len[m], (int64_t)N);
+          if (hi > lo) bytes += (uint32_t)(hi - lo) * kTileNodeBytes;
+        }
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&full[st])),
+                     "r"(bytes)
+                     : "memory");
+        bulk_g2s(sb, tcode + r0 * 32, kStageCodes, &full[st]);
+        if (vbytes) bulk_g2s(sb + kStageCodes, tv + kValPad * base + (int64_t)h * (16 * kValPad) * len, vbytes,
+                             &full[st]);
+        double* xs = reinterpret_cast<double*>(sb + kStageCodes + kStageVals);
+        for (int m = 0; m < T.nrange; ++m) {
+          // the runs clipped to the mesh; nodes outside it are never named by a code
+          const int64_t lo = max(r0 + T.a[m], (int64_t)0), hi = min(r0 + T.a[m] + T.len[m], (int64_t)N);
+          if (hi > lo)
+            bulk_g2s(xs + (int64_t)(T.sb[m] + (lo - (r0 + T.a[m]))) * (3 * kTileNr), x + lo * (3 * kTileNr),
+                     (uint32_t)(hi - lo) * kTileNodeBytes, &full[st]);
+        }
+      }
+    }
+  } else {
+    const int rl = threadIdx.x >> 3;
+    const int k0 = (threadIdx.x & 7) * 2;
+    int k = 0;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++k) {
+      const int st = k & 1;
+      const unsigned char* sb = tsm + st * stage_bytes;
+      const int64_t sl = tile >> 1;
+      const int64_t row = sl * kSlice + (tile & 1) * kTileRows + rl;
+      const int len = (int)((sptr[sl + 1] - sptr[sl]) >> 5);
+      double acc[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+      if (!mbar_wait(&full[st], (uint32_t)(k >> 1) & 1u)) late = true;
+      const uint32_t* cw = reinterpret_cast<const uint32_t*>(sb) + rl * 8;
+      const double* vs = reinterpret_cast<const double*>(sb + kStageCodes) + rl * kValPad;
+      const double* xs = reinterpret_cast<const double*>(sb + kStageCodes + kStageVals) + k0;
+      // rows past the mesh (last tile only) have no blocks; in a real row every
+      // step below len names a block (padding blocks: the row itself, zero values)
+      const int rlen = row < N ? len : 0;
+      auto step = [&](unsigned nd, int j) {
+        const double2* v2 = reinterpret_cast<const double2*>(vs + j * (16 * kValPad));
+        double mv[10];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          const double2 w = v2[q];
+          mv[2 * q] = w.x;
+          mv[2 * q + 1] = w.y;
+        }
+        const double* xp = xs + nd * (3 * kTileNr);
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) {
+          const double2 xv = *reinterpret_cast<const double2*>(xp + comp * kTileNr);
+          acc[0][0] += mv[comp] * xv.x;
+          acc[0][1] += mv[comp] * xv.y;
+          acc[1][0] += mv[3 + comp] * xv.x;
+          acc[1][1] += mv[3 + comp] * xv.y;
+          acc[2][0] += mv[6 + comp] * xv.x;
+          acc[2][1] += mv[6 + comp] * xv.y;
+        }
+      };
+      int j = 0;
+#pragma unroll 1
+      for (; j + 4 <= rlen; j += 4) {
+        const uint32_t w = cw[j >> 2];
+        step(w & 0xFFu, j);
+        step((w >> 8) & 0xFFu, j + 1);
+        step((w >> 16) & 0xFFu, j + 2);
+        step(w >> 24, j + 3);
+      }
+      if (j < rlen) {
+        const uint32_t w = cw[j >> 2];
+        step(w & 0xFFu, j);
+        if (j + 1 < rlen) step((w >> 8) & 0xFFu, j + 1);
+        if (j + 2 < rlen) step((w >> 16) & 0xFFu, j + 2);
+      }
+      // the stage is free once every consumer warp has read it
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[st])) : "memory");
+      if (row < N) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          st_g<2>(y + (3 * row + r) * kTileNr + k0, acc[r]);
+          if (MODE == 1) {
+            double xr[2];
+            ldg_g<2>(x + (3 * row + r) * kTileNr + k0, xr);
+            dot[0][0] += xr[0] * acc[r][0];
+            dot[0][1] += xr[1] * acc[r][1];
+          }
+        }
+      }
+    }
+  }
+  if (late) atomicOr(err, kDevTimeout);
+  if (MODE == 1) {
+    double tot[1];
+    if (rhs_grid_sum<2, 1, kTileBlk>(dot, kTileNr / 2, kTileNr, partials, &s->ticket[0], tot)) {
+      const int kk = threadIdx.x;
+      const bool ok = s->active[kk] && fabs(tot[0]) > 1e-300 && isfinite(tot[0]);
+      s->alpha[kk] = ok ? s->rz[kk] / tot[0] : 0.0;
+      if (s->active[kk] && !ok) s->active[kk] = 0;  // breakdown of this rhs
+    }
+  } else {
+    __syncthreads();  // no block leaves while copies into its stages may be in flight
+  }
+}
+
 // x += alpha p, r -= alpha q, then r.z and r.r per rhs, beta and the stop tests.
 template <int G>
 __global__ void __launch_bounds__(kBlk)
@@ -556,7 +796,59 @@ struct BlockRun {
   BScalars* s;
   double* partials;
   int g_spmv, g_vec;
+  bool tile;  // k_bspmv_tile (16 rhs, coded full storage)
+  BTile T;
+  int g_tile;
+  double* tv;   // values in tile order (k_tile_vals)
+  uint8_t* tc;  // codes in tile form (k_tile_codes)
 };
+
+// The tile of k_bspmv_tile from the offsets of the coded storage (ascending);
+// false when the pattern's tile would not fit three blocks per SM.
+bool make_tile(const Ctx* c, BTile* T) {
+  *T = BTile{};
+  if (!c->full_coded || c->full_ntab <= 0) return false;
+  int m = -1;
+  std::vector<int> run(c->full_ntab);
+  for (int k = 0; k < c->full_ntab; ++k) {
+    const int a = c->full_tab.off[k];
+    if (m >= 0 && a <= T->a[m] + T->len[m]) {
+      T->len[m] = std::max(T->len[m], a + kTileRows - T->a[m]);
+    } else {
+      ++m;
+      T->a[m] = a;
+      T->len[m] = kTileRows;
+    }
+    run[k] = m;
+  }
+  T->nrange = m + 1;
+  int nodes = 0;
+  for (int q = 0; q < T->nrange; ++q) {
+    T->sb[q] = nodes;
+    nodes += T->len[q];
+  }
+  T->nodes = nodes;
+  for (int k = 0; k < c->full_ntab; ++k) T->node0[k] = T->sb[run[k]] + (c->full_tab.off[k] - T->a[run[k]]);
+  return nodes <= kTileMaxNodes;
+}
+
+void launch_bspmv_tile(const BlockRun& B, cudaStream_t st, int mode, const double* x, double* y) {
+  Ctx* c = B.c;
+  const size_t sm = 2 * tile_stage_bytes(B.T.nodes);
+  if (mode == 1)
+    k_bspmv_tile<1><<<B.g_tile, kTileBlk, sm, st>>>(c->N, c->nslices, c->slice_ptr, B.tc, B.tv, B.T, x, y, B.s,
+                                                    B.partials, c->dev_err);
+  else
+    k_bspmv_tile<0><<<B.g_tile, kTileBlk, sm, st>>>(c->N, c->nslices, c->slice_ptr, B.tc, B.tv, B.T, x, y, B.s,
+                                                    B.partials, c->dev_err);
+}
+
+cudaError_t prepare_tile(const BTile& T) {
+  const int sm = (int)(2 * tile_stage_bytes(T.nodes));
+  cudaError_t e = cudaFuncSetAttribute(k_bspmv_tile<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_bspmv_tile<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  return e;
+}
 
 template <int RPW>
 void launch_bspmv_pipe(const BlockRun& B, cudaStream_t st, int mode, const double* x, double* y) {
@@ -596,6 +888,10 @@ template <int G>
 void launch_bspmv(const BlockRun& B, cudaStream_t st, int mode, const double* x, double* y) {
   Ctx* c = B.c;
   if constexpr (G == 2) {
+    if (B.tile) {
+      launch_bspmv_tile(B, st, mode, x, y);
+      return;
+    }
     // 4..32 right-hand sides: the pipelined kernel (rows per warp task = 32 / tpr)
     switch (B.tpr) {
       case 2: launch_bspmv_pipe<16>(B, st, mode, x, y); return;
@@ -746,11 +1042,15 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* Bm, double* X, const ufc_sol
   B.dinv = algo->precond_type == UFC_SOLV_PREC_JACOBI ? c->dinv64 : nullptr;
   B.g_spmv = grid_blocks(c->nslices * B.tpr * 32);
   if (G == 2) UFC_CUDA(c, prepare_bspmv(B.tpr));
+  B.tile = nr == kTileNr && make_tile(c, &B.T);
+  B.g_tile = (int)std::min<int64_t>(2 * c->nslices, (int64_t)sm_count());
+  if (B.tile) UFC_CUDA(c, prepare_tile(B.T));
   B.g_vec = grid_blocks(c->n * B.tpr);
   BScalars* hs = nullptr;
   int32_t* restart_dev = nullptr;
   auto cleanup = [&]() {
     dfree(&B.bx); dfree(&B.xx); dfree(&B.rx); dfree(&B.px); dfree(&B.qx); dfree(&B.s); dfree(&B.partials);
+    dfree(&B.tv); dfree(&B.tc);
     dfree(&restart_dev);
     if (hs) cudaFreeHost(hs);
     hs = nullptr;
@@ -775,8 +1075,17 @@ int pcg_solve_block(Ctx* c, int nrhs, const double* Bm, double* X, const ufc_sol
   BCUDA(cudaMemsetAsync(B.px, 0, sizeof(double) * B.nn, c->stream));
   BTRY(dalloc(c, &B.qx, B.nn));
   BTRY(dalloc(c, &B.s, 1));
-  BTRY(dalloc(c, &B.partials, (int64_t)std::max(B.g_spmv, B.g_vec) * kNvMax * kMaxRhs));
+  BTRY(dalloc(c, &B.partials, (int64_t)std::max({B.g_spmv, B.g_vec, B.g_tile}) * kNvMax * kMaxRhs));
   BTRY(dalloc(c, &restart_dev, kMaxRhs));
+  if (B.tile) {
+    BTRY(dalloc(c, &B.tv, kValPad * c->sell_blocks));
+    const int64_t rows = c->nslices * kSlice;
+    k_tile_vals<<<(int)((rows + 255) / 256), 256, 0, c->stream>>>(rows, c->slice_ptr, c->val64, B.tv);
+    BCUDA(cudaGetLastError());
+    BTRY(dalloc(c, &B.tc, rows * 32));
+    k_tile_codes<<<(int)((rows * 32 + 255) / 256), 256, 0, c->stream>>>(rows, c->full_code, B.T, B.tc);
+    BCUDA(cudaGetLastError());
+  }
   BCUDA(cudaMallocHost((void**)&hs, sizeof(BScalars)));
   cudaEvent_t t0, t1;
   BCUDA(cudaEventCreate(&t0));

@@ -40,6 +40,7 @@ int check_dev_err(Ctx* c, const char* where) {
   if (e & kDevValence) m += " a node is shared by more than 32 elements;";
   if (e & kDevRowBlocks) m += " a node couples to more than 128 nodes;";
   if (e & kDevPattern) m += " element block missing from the pattern;";
+  if (e & kDevTimeout) m += " a bounded wait for an asynchronous copy gave up;";
   cudaMemsetAsync(c->dev_err, 0, sizeof(int32_t), c->stream);
   return fail(c, UFC_STATUS_ERROR, m);
 }

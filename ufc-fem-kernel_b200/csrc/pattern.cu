@@ -556,6 +556,7 @@ int build_full_codes(Ctx* c) {
     return done(UFC_STATUS_OK);
   }
   c->full_tab = tab;
+  c->full_ntab = ntab;
   c->full_coded = true;
   return done(UFC_STATUS_OK);
 }

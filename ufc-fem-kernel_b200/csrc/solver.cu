@@ -234,27 +234,6 @@ __global__ void __launch_bounds__(kSpmvBlock)
   }
 }
 
-// 32 code bytes of one row, consumed from the front one block step at a time.
-struct Code256 {
-  uint64_t w0, w1, w2, w3;
-  __device__ __forceinline__ unsigned front() const { return (unsigned)(w0 & 0xFFu); }
-  template <int B>
-  __device__ __forceinline__ void drop() {
-    if constexpr (B >= 8) {
-      w0 = w1;
-      w1 = w2;
-      w2 = w3;
-      w3 = 0;
-    } else {
-      constexpr int sh = 8 * B;
-      w0 = (w0 >> sh) | (w1 << (64 - sh));
-      w1 = (w1 >> sh) | (w2 << (64 - sh));
-      w2 = (w2 >> sh) | (w3 << (64 - sh));
-      w3 >>= sh;
-    }
-  }
-};
-
 // y = K x on the full SELL storage with coded indices (see build_full_codes):
 // each row loads its 32 code bytes with two 16-byte loads when the warp
 // starts, and block j's column is row + off[code j], so no column index is

@@ -56,6 +56,28 @@ enum DevErr : int32_t {
   kDevValence = 4,
   kDevRowBlocks = 8,
   kDevPattern = 16,
+  kDevTimeout = 32,  // a bounded wait (mbarrier) gave up
+};
+
+// 32 code bytes of one row, consumed from the front one block step at a time.
+struct Code256 {
+  uint64_t w0, w1, w2, w3;
+  __device__ __forceinline__ unsigned front() const { return (unsigned)(w0 & 0xFFu); }
+  template <int B>
+  __device__ __forceinline__ void drop() {
+    if constexpr (B >= 8) {
+      w0 = w1;
+      w1 = w2;
+      w2 = w3;
+      w3 = 0;
+    } else {
+      constexpr int sh = 8 * B;
+      w0 = (w0 >> sh) | (w1 << (64 - sh));
+      w1 = (w1 >> sh) | (w2 << (64 - sh));
+      w2 = (w2 >> sh) | (w3 << (64 - sh));
+      w3 >>= sh;
+    }
+  }
 };
 
 struct Mg;  // multigrid hierarchy (mg.cu)
@@ -143,6 +165,7 @@ struct Ctx {
   // 31 distinct offsets): 32 code bytes per row, lane-major
   bool full_coded = false;
   FullOffsets full_tab{};
+  int32_t full_ntab = 0;  // offsets in full_tab (ascending)
   uint8_t* full_code = nullptr;          // [nslices * 32 * 32]
   SymOffsets sym_tab{};
   uint8_t* sym_ucode = nullptr;          // [nslices * 32 * 16]
