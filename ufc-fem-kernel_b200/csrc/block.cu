@@ -472,8 +472,9 @@ __global__ void k_tile_codes(int64_t rows, const uint8_t* __restrict__ code, con
 // per node), so that every x line of a tile crosses L2 once.  The 128
 // consumer threads (8 per row, 2 rhs each) multiply from shared memory while
 // the next tile lands, then release the stage; a step costs them one byte
-// extract, one address and eight 16-byte shared loads besides the 18 FMAs.  The same products in the same order as k_bspmv_pipe, so the same y.
-// Every wait is bounded; a wait that gives up sets kDevTimeout.
+// extract, one address and eight 16-byte shared loads besides the 18 FMAs.
+// The same products in the same order as k_bspmv_pipe, so the same y.  Every
+// wait is bounded; a wait that gives up sets kDevTimeout.
 template <int MODE>
 __global__ void __launch_bounds__(kTileBlk, 1)
     k_bspmv_tile(int32_t N, int64_t nslices, const int64_t* __restrict__ sptr, const uint8_t* __restrict__ tcode,
