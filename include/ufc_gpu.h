@@ -379,6 +379,13 @@ int ufc_bc_set(ufc_ctx* ctx, const ufc_bc_desc* bc);
  * element colouring of RT_AsmColor_Build (ufc_core/L5_RT/Assembly/RT_Asm_Color.f90:36-182). */
 int ufc_pattern_build(ufc_ctx* ctx, ufc_pattern_info* info);
 int ufc_csr_export(ufc_ctx* ctx, const ufc_csr_export_arg* arg);
+/* The element colours of the last ufc_pattern_build: RT_AsmColorResult%color_of
+ * of RT_AsmColor_Build (ufc_core/L5_RT/Assembly/RT_Asm_Color.f90:36-182), the
+ * greedy colouring (elements in ascending order, each the smallest colour that
+ * no lower-numbered element sharing a node has), computed on the device.
+ * color_of[e] lies in index_base .. index_base + n_colors - 1 (index_base 1 gives
+ * the reference's 1-based colours); mem: memory of color_of ([n_elems]). */
+int ufc_pattern_colors(ufc_ctx* ctx, int32_t* color_of, int32_t index_base, int32_t mem);
 
 /* ---- element / material ---- */
 int ufc_elem_compute_ke(ufc_ctx* ctx, ufc_elem_ke_arg* arg);

@@ -147,7 +147,7 @@ MODULE ufc_gpu_brg
   PUBLIC :: ufc_ctx_set_stream, ufc_ctx_set_instrument, ufc_stress_eval, ufc_spmv, ufc_mg_level_info
   PUBLIC :: ufc_mg_export, ufc_last_timing, ufc_last_residual_history, ufc_set_displacement, ufc_get_state
   PUBLIC :: ufc_csr_spmv_dot_noalloc
-  PUBLIC :: ufc_pattern_build, ufc_csr_export, ufc_elem_compute_ke, ufc_elem_compute_fint
+  PUBLIC :: ufc_pattern_build, ufc_csr_export, ufc_pattern_colors, ufc_elem_compute_ke, ufc_elem_compute_fint
   PUBLIC :: ufc_mat_update_batch, ufc_pcg_solve, ufc_pcg_solve_block, ufc_nr_increment
   PUBLIC :: ufc_state_commit, ufc_state_rollback, ufc_get_displacement, ufc_adjoint_sensitivity
   PUBLIC :: ufc_nr_step, ufc_load_faces, ufc_stress_nodal, ufc_reactions, ufc_mg_setup, ufc_mg_apply
@@ -192,6 +192,14 @@ MODULE ufc_gpu_brg
       IMPORT :: C_INT, C_PTR, ufc_csr_export_arg
       TYPE(C_PTR), VALUE                   :: ctx
       TYPE(ufc_csr_export_arg), INTENT(IN) :: arg
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION ufc_pattern_colors(ctx, color_of, index_base, mem) &
+        BIND(C, NAME='ufc_pattern_colors')
+      IMPORT :: C_INT, C_PTR, C_INT32_T
+      TYPE(C_PTR), VALUE               :: ctx
+      INTEGER(C_INT32_T), INTENT(OUT)  :: color_of(*)
+      INTEGER(C_INT32_T), VALUE        :: index_base
+      INTEGER(C_INT32_T), VALUE        :: mem
     END FUNCTION
     INTEGER(C_INT) FUNCTION ufc_elem_compute_ke(ctx, arg) BIND(C, NAME='ufc_elem_compute_ke')
       IMPORT :: C_INT, C_PTR, ufc_elem_ke_arg

@@ -3,6 +3,8 @@
 Pattern and index work are compared bit for bit; FP64 values to 1e-12
 relative; solutions to the tolerances stated in each test.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -33,6 +35,40 @@ def test_pattern_bit_exact(pkg, orc, name, make):
     assert np.array_equal(col, col_o)
     rp1, col1, _, _ = m.csr_export(index_base=1)
     assert rp1[0] == 1 and np.array_equal(rp1 - 1, rp_o) and np.array_equal(col1 - 1, col_o)
+
+
+def _shuffled_elements(p, seed):
+    """The same problem with its elements listed in a random order."""
+    perm = np.random.default_rng(seed).permutation(p.n_elems)
+    return dataclasses.replace(p, name=p.name + "_shuffled", conn=np.ascontiguousarray(p.conn[perm]),
+                               props=np.ascontiguousarray(p.props[perm]))
+
+
+COLOURED = [
+    ("cantilever_40x8x8", lambda mesh: mesh.config1()),
+    ("lognormal_24x12x12", lambda mesh: mesh.lognormal_cantilever(24, 12, 12, seed=4)),
+    ("shuffled_12x6x6", lambda mesh: _shuffled_elements(mesh.cantilever(12, 6, 6, 12.0, 6.0, 6.0), 7)),
+    ("shuffled_10x2x2", lambda mesh: _shuffled_elements(mesh.config1(), 3)),
+    ("strip_3000x1x1", lambda mesh: mesh.cantilever(3000, 1, 1, 3000.0, 1.0, 1.0)),
+    ("strip_6000x1x1", lambda mesh: mesh.cantilever(6000, 1, 1, 6000.0, 1.0, 1.0)),
+]
+
+
+@pytest.mark.parametrize("name,make", COLOURED)
+def test_element_colours_match_oracle(pkg, orc, name, make):
+    """ufc_pattern_build colours the elements on the device by in-place sweeps
+    of the greedy map; the colours equal the oracle's sequential greedy
+    colouring (RT_AsmColor_Build) element for element, on structured and
+    shuffled element orders and on strips one element thick, whose chains of
+    lower neighbours are as long as the strip (the longer one may exceed the
+    sweep limit, after which the host colouring finishes: the same colours)."""
+    p = make(pkg.mesh)
+    m = pkg.FemModel.from_problem(p)
+    ref, ncol = orc.color_elements(p.n_nodes, p.conn)
+    assert m.info.n_colors == ncol
+    assert np.array_equal(m.colors(), ref)
+    assert np.array_equal(m.colors(index_base=1), ref + 1)
+    m.close()
 
 
 @pytest.mark.parametrize("name,make", SMALL)

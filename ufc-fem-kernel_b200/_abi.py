@@ -152,6 +152,7 @@ _SIGS = {
     "ufc_bc_set": [_p, C.POINTER(BcDesc)],
     "ufc_pattern_build": [_p, C.POINTER(PatternInfo)],
     "ufc_csr_export": [_p, C.POINTER(CsrExportArg)],
+    "ufc_pattern_colors": [_p, _p, _i32, _i32],
     "ufc_elem_compute_ke": [_p, C.POINTER(ElemKeArg)],
     "ufc_elem_compute_fint": [_p, C.POINTER(ElemFeArg)],
     "ufc_mat_update_batch": [_p, C.POINTER(MatUpdateArg)],

@@ -434,6 +434,23 @@ int ufc_csr_export(ufc_ctx* c, const ufc_csr_export_arg* a) {
   return sync(c);
 }
 
+int ufc_pattern_colors(ufc_ctx* c, int32_t* color_of, int32_t index_base, int32_t mem) {
+  CTX_CHECK(c);
+  if (!c->has_pattern) return fail(c, UFC_STATUS_INVALID, "ufc_pattern_colors: pattern not built");
+  if (!color_of || (index_base != 0 && index_base != 1))
+    return fail(c, UFC_STATUS_INVALID, "ufc_pattern_colors: NULL color_of or index_base not 0 or 1");
+  Scope sc(c);
+  std::vector<int32_t> h(c->h_color);
+  for (int32_t& v : h) v += index_base;
+  if (mem == UFC_MEM_DEVICE) {
+    UFC_CUDA(c, cudaMemcpyAsync(color_of, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  } else {
+    std::copy(h.begin(), h.end(), color_of);
+  }
+  return sync(c);
+}
+
 int ufc_elem_compute_ke(ufc_ctx* c, ufc_elem_ke_arg* a) {
   CTX_CHECK(c);
   if (!a || (a->build & (UFC_BUILD_FP64 | UFC_BUILD_FP32 | UFC_BUILD_FP32_ROUNDED | UFC_BUILD_FP32_DIFF |

@@ -14,7 +14,8 @@
 //
 // Element colouring for the deterministic scatter is the greedy colouring of
 // RT_AsmColor_Build (ufc_core/L5_RT/Assembly/RT_Asm_Color.f90:36-182), elements
-// visited in ascending order, smallest free colour first.
+// visited in ascending order, smallest free colour first; it is computed on the
+// device as the fixed point of that rule (k_color_sweep).
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
@@ -62,6 +63,83 @@ __global__ void k_sort_node_elems(int32_t N, const int32_t* __restrict__ nptr, i
       --j;
     }
     nlst[b + j + 1] = v;
+  }
+}
+
+// Element colouring on the device.  The sequential greedy colouring (elements
+// in ascending order, each taking the smallest colour that none of its lower
+// neighbours -- elements f < e sharing a node with e -- has) is the unique
+// fixed point of the map colour[e] = mex{colour[f] : f a lower neighbour of e}:
+// element 0 has no lower neighbour, and by induction every element is fixed
+// once its lower neighbours are.  Sweeping that map over all elements at once,
+// in place, from colour 0 everywhere therefore reaches exactly the sequential
+// colouring, and a sweep that changes nothing proves it has been reached (every
+// element then read values that did not move).  The number of sweeps follows
+// the longest chain of lower neighbours along which the colours still change:
+// about nx + ny + nz on a structured box numbered lexicographically, fewer on
+// shuffled numberings.
+
+// Lower neighbours of element e, ascending and unique: an 8-way merge of its
+// nodes' element lists (sorted by k_sort_node_elems), stopped at e itself.
+// kFill = false counts them into cnt[e], true writes them at elst + eptr[e].
+template <bool kFill>
+__global__ void __launch_bounds__(128)
+    k_elem_lower(int32_t E, const int32_t* __restrict__ conn, const int32_t* __restrict__ nptr,
+                 const int32_t* __restrict__ nlst, int64_t* __restrict__ cnt, const int64_t* __restrict__ eptr,
+                 int32_t* __restrict__ elst) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  int32_t pos[8], end[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int32_t nd = conn[e * 8 + a];
+    pos[a] = nptr[nd];
+    end[a] = nptr[nd + 1];
+  }
+  int32_t* out = kFill ? elst + eptr[e] : nullptr;
+  int64_t m = 0;
+  for (;;) {
+    int32_t best = INT32_MAX;
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      if (pos[a] < end[a]) best = min(best, nlst[pos[a]]);
+    if (best >= e) break;  // every list holds e itself; what follows it is higher
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      if (pos[a] < end[a] && nlst[pos[a]] == best) ++pos[a];
+    if (kFill) out[m] = best;
+    ++m;
+  }
+  if (!kFill) cnt[e] = m;
+}
+
+// One in-place sweep of the colouring map.  flag[0] is set when a colour moved,
+// flag[1] when a mex exceeded 255 (impossible while a node has at most
+// kMaxValence elements: an element then has at most 8 (kMaxValence - 1) lower
+// neighbours; the host colouring takes over if it happens).  Reads of colours
+// other threads write in the same sweep see either value, both of which the
+// fixed-point argument allows.
+__global__ void __launch_bounds__(256)
+    k_color_sweep(int32_t E, const int64_t* __restrict__ eptr, const int32_t* __restrict__ elst,
+                  uint8_t* color, int32_t* __restrict__ flag) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  uint64_t used[4] = {0, 0, 0, 0};
+  for (int64_t k = eptr[e]; k < eptr[e + 1]; ++k) {
+    const unsigned cf = color[elst[k]];
+    used[cf >> 6] |= 1ull << (cf & 63);
+  }
+  unsigned c = 256;
+#pragma unroll
+  for (int w = 3; w >= 0; --w)
+    if (~used[w]) c = 64 * w + __ffsll((long long)~used[w]) - 1;
+  if (c > 255) {
+    flag[1] = 1;
+    return;
+  }
+  if (color[e] != c) {
+    color[e] = (uint8_t)c;
+    flag[0] = 1;
   }
 }
 
@@ -408,7 +486,9 @@ __global__ void k_export(int32_t N, const int32_t* __restrict__ brow, const int3
   }
 }
 
-// Greedy colouring on the host (deterministic, visits elements in order).
+// Greedy colouring on the host (deterministic, visits elements in order): the
+// same colouring as the device sweeps, used only when they have not settled
+// within kMaxColorSweeps.
 int color_elements(Ctx* c, std::vector<int32_t>& color) {
   const int32_t N = c->N, E = c->E;
   const std::vector<int32_t>& conn = c->h_conn;
@@ -449,6 +529,77 @@ int scan_exclusive(Ctx* c, const T* in, T* out, int64_t n) {
   cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, c->stream);
   cudaFreeAsync(tmp, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "cub::DeviceScan::ExclusiveSum");
+  return UFC_STATUS_OK;
+}
+
+// Sweeps launched between two looks at their flags, and the number after which
+// the host colouring takes over (numberings whose lower-neighbour chains keep
+// changing colours for that long, e.g. a strip one element thick numbered
+// along its length, which settles one element per sweep).
+constexpr int kColorBatch = 32;
+constexpr int kMaxColorSweeps = 4096;
+
+struct ColorTmp {
+  int64_t* cnt = nullptr;
+  int64_t* eptr = nullptr;
+  int32_t* elst = nullptr;
+  uint8_t* col8 = nullptr;
+  int32_t* flags = nullptr;
+  ~ColorTmp() {
+    dfree(&cnt);
+    dfree(&eptr);
+    dfree(&elst);
+    dfree(&col8);
+    dfree(&flags);
+  }
+};
+
+// The greedy colouring of RT_AsmColor_Build (RT_Asm_Color.f90:36-182) by
+// in-place sweeps on the device (see k_color_sweep) over the lower-neighbour
+// lists, from the node -> element lists nptr / nlst; color[e] on the host.
+int color_elements_device(Ctx* c, const int32_t* nptr, const int32_t* nlst, std::vector<int32_t>& color) {
+  const int32_t E = c->E;
+  ColorTmp t;
+  UFC_TRY(dalloc(c, &t.cnt, (int64_t)E + 1));
+  UFC_TRY(dalloc(c, &t.eptr, (int64_t)E + 1));
+  UFC_CUDA(c, cudaMemsetAsync(t.cnt + E, 0, sizeof(int64_t), c->stream));
+  k_elem_lower<false><<<grid_for(E, 128), 128, 0, c->stream>>>(E, c->conn, nptr, nlst, t.cnt, nullptr, nullptr);
+  UFC_CUDA(c, cudaGetLastError());
+  UFC_TRY(scan_exclusive(c, t.cnt, t.eptr, (int64_t)E + 1));
+  int64_t total = 0;
+  UFC_CUDA(c, cudaMemcpyAsync(&total, t.eptr + E, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  UFC_TRY(dalloc(c, &t.elst, total));
+  k_elem_lower<true><<<grid_for(E, 128), 128, 0, c->stream>>>(E, c->conn, nptr, nlst, nullptr, t.eptr, t.elst);
+  UFC_CUDA(c, cudaGetLastError());
+  UFC_TRY(dalloc(c, &t.col8, E));
+  UFC_TRY(dalloc(c, &t.flags, 2 * kColorBatch));
+  UFC_CUDA(c, cudaMemsetAsync(t.col8, 0, (size_t)E, c->stream));
+  int32_t hf[2 * kColorBatch];
+  bool settled = false, overflow = false;
+  for (int sweeps = 0; !settled && !overflow && sweeps < kMaxColorSweeps; sweeps += kColorBatch) {
+    UFC_CUDA(c, cudaMemsetAsync(t.flags, 0, sizeof(int32_t) * 2 * kColorBatch, c->stream));
+    for (int b = 0; b < kColorBatch; ++b)
+      k_color_sweep<<<grid_for(E, 256), 256, 0, c->stream>>>(E, t.eptr, t.elst, t.col8, t.flags + 2 * b);
+    UFC_CUDA(c, cudaGetLastError());
+    UFC_CUDA(c, cudaMemcpyAsync(hf, t.flags, sizeof(hf), cudaMemcpyDeviceToHost, c->stream));
+    UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int b = 0; b < kColorBatch && !settled; ++b) {
+      overflow |= hf[2 * b + 1] != 0;
+      settled = hf[2 * b] == 0 && hf[2 * b + 1] == 0;
+    }
+  }
+  if (!settled) return color_elements(c, color);
+  std::vector<uint8_t> h((size_t)E);
+  UFC_CUDA(c, cudaMemcpyAsync(h.data(), t.col8, (size_t)E, cudaMemcpyDeviceToHost, c->stream));
+  UFC_CUDA(c, cudaStreamSynchronize(c->stream));
+  color.resize(E);
+  int ncol = 0;
+  for (int32_t e = 0; e < E; ++e) {
+    color[e] = h[e];
+    ncol = std::max(ncol, (int)h[e] + 1);
+  }
+  c->ncol = ncol;
   return UFC_STATUS_OK;
 }
 
@@ -570,22 +721,7 @@ int build_pattern(Ctx* c) {
   c->has_sym_pattern = c->has_sval64 = c->has_sval32 = c->sym_coded = false;
   const int32_t N = c->N, E = c->E;
 
-  // 1. colouring (host) and colour-grouped element lists
-  std::vector<int32_t> color;
-  UFC_TRY(color_elements(c, color));
-  c->h_color = color;
-  c->col_off.assign(c->ncol + 1, 0);
-  for (int32_t e = 0; e < E; ++e) c->col_off[color[e] + 1]++;
-  for (int k = 0; k < c->ncol; ++k) c->col_off[k + 1] += c->col_off[k];
-  {
-    std::vector<int32_t> lst(E), fill(c->col_off.begin(), c->col_off.end() - 1);
-    for (int32_t e = 0; e < E; ++e) lst[fill[color[e]]++] = e;
-    UFC_TRY(dalloc(c, &c->col_elems, E));
-    UFC_CUDA(c, cudaMemcpyAsync(c->col_elems, lst.data(), sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream));
-    UFC_CUDA(c, cudaStreamSynchronize(c->stream));
-  }
-
-  // 2. node -> element adjacency on the device
+  // 1. node -> element adjacency on the device
   int32_t *cnt = nullptr, *nptr = nullptr, *fill = nullptr, *nlst = nullptr;
   UFC_TRY(dalloc(c, &cnt, (int64_t)N + 1));
   UFC_TRY(dalloc(c, &nptr, (int64_t)N + 1));
@@ -603,6 +739,33 @@ int build_pattern(Ctx* c) {
   if (st != UFC_STATUS_OK) {
     dfree(&cnt); dfree(&nptr); dfree(&fill); dfree(&nlst);
     return st;
+  }
+
+  // 2. colouring (device sweeps) and colour-grouped element lists
+  {
+    std::vector<int32_t> color;
+    st = color_elements_device(c, nptr, nlst, color);
+    if (st != UFC_STATUS_OK) {
+      dfree(&cnt); dfree(&nptr); dfree(&fill); dfree(&nlst);
+      return st;
+    }
+    c->col_off.assign(c->ncol + 1, 0);
+    for (int32_t e = 0; e < E; ++e) c->col_off[color[e] + 1]++;
+    for (int k = 0; k < c->ncol; ++k) c->col_off[k + 1] += c->col_off[k];
+    std::vector<int32_t> lst(E), pos(c->col_off.begin(), c->col_off.end() - 1);
+    for (int32_t e = 0; e < E; ++e) lst[pos[color[e]]++] = e;
+    c->h_color = std::move(color);
+    st = dalloc(c, &c->col_elems, E);
+    if (st == UFC_STATUS_OK) {
+      cudaError_t ce =
+          cudaMemcpyAsync(c->col_elems, lst.data(), sizeof(int32_t) * E, cudaMemcpyHostToDevice, c->stream);
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(c->stream);
+      if (ce != cudaSuccess) st = cuda_fail(c, ce, "ufc_pattern_build (colour lists)");
+    }
+    if (st != UFC_STATUS_OK) {
+      dfree(&cnt); dfree(&nptr); dfree(&fill); dfree(&nlst);
+      return st;
+    }
   }
 
   // 3. block rows: count, scan, fill

@@ -232,6 +232,14 @@ class FemModel:
         return {"n_dof": info.n_dof, "nnz": info.nnz, "nnzb": info.nnzb, "sell_blocks": info.sell_blocks,
                 "n_colors": info.n_colors, "max_row_blocks": info.max_row_blocks}
 
+    def colors(self, index_base=0):
+        """Element colours of the pattern build (RT_AsmColorResult%color_of of
+        RT_AsmColor_Build), int32 on the host."""
+        out = np.zeros(self.n_elems, dtype=np.int32)
+        self._check(self.lib.ufc_pattern_colors(self.h, out.ctypes.data, int(index_base), A.MEM_HOST),
+                    "ufc_pattern_colors")
+        return out
+
     @classmethod
     def from_problem(cls, p, device=0, build_pattern=True, lib=None):
         """Model of a `mesh.Problem` (mesh, material, Dirichlet set)."""
