@@ -74,3 +74,22 @@ def test_newton_increment_and_step_driver(pkg, orc):
                                             max_cutbacks=1)
     assert status.status_code == api.IF_STATUS_NOT_CONVERGED and res is not None and not res.completed
     ctx.model.close()
+
+
+def test_rt_asmcolor_build_matches_oracle(pkg, orc):
+    """RT_AsmColor_Build returns the device colouring with the reference's
+    1-based colours and its colour groups; the colours are the oracle's greedy
+    colouring plus one, and the groups list every element once, by colour."""
+    api = pkg.ufc_api
+    p = pkg.mesh.lognormal_cantilever(12, 6, 6, seed=2)
+    ctx = api.NM_Solver_Ctx(pkg.FemModel.from_problem(p))
+    res = api.RT_AsmColor_Result()
+    status = api.RT_AsmColor_Build(ctx, res)
+    assert status.ok
+    ref, ncol = orc.color_elements(p.n_nodes, p.conn)
+    assert res.n_colors == ncol and np.array_equal(res.color_of, ref + 1)
+    assert res.color_count.sum() == p.n_elems and res.color_start[-1] == p.n_elems + 1
+    for c in range(ncol):
+        grp = res.color_elems[res.color_start[c] - 1:res.color_start[c + 1] - 1]
+        assert np.array_equal(grp, np.flatnonzero(ref == c) + 1)
+    ctx.model.close()

@@ -37,3 +37,26 @@ def test_pcg_rejects_missing_rhs_without_a_device(pkg):
     status = api.NM_Solver_PCG(api.NM_Solver_Desc(n=10), api.NM_Solver_State(b=[0.0] * 9), api.NM_Solver_Algo(),
                                api.NM_Solver_Ctx(NoModel()))
     assert status.status_code == api.IF_STATUS_INVALID and "desc%n" in status.message
+
+
+def test_color_groups_follow_build_color_groups(pkg):
+    """The colour groups of RT_AsmColor_Build (build_color_groups,
+    RT_Asm_Color.f90:148-180), restated as its loops, against ufc_api's
+    vectorised form on a random 1-based colouring."""
+    import numpy as np
+
+    color_of = np.random.default_rng(3).integers(1, 9, size=500).astype(np.int32)
+    n = int(color_of.max())
+    count = [0] * n
+    for c in color_of:
+        count[c - 1] += 1
+    start = [1] * (n + 1)
+    for c in range(n):
+        start[c + 1] = start[c] + count[c]
+    elems, fill = [0] * len(color_of), [0] * n
+    for ie, c in enumerate(color_of, start=1):
+        elems[start[c - 1] + fill[c - 1] - 1] = ie
+        fill[c - 1] += 1
+    got = pkg.ufc_api.color_groups(color_of)
+    assert got[0] == n
+    assert got[1].tolist() == count and got[2].tolist() == start and got[3].tolist() == elems

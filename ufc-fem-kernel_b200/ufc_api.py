@@ -199,6 +199,44 @@ def PH_Element_Compute_Fe(ctx: NM_Solver_Ctx, arg: PH_Element_Compute_Fe_Arg) ->
 
 
 # ---------------------------------------------------------------- L5 assembly and nonlinear driver
+@dataclass
+class RT_AsmColor_Result:
+    """RT_AsmColor_Result (ufc_core/L5_RT/Assembly/RT_Asm_Color.f90:26-32), with
+    the reference's 1-based colours and element ids."""
+    color_of: np.ndarray | None = None     # [n_elem] colour of each element, 1..n_colors
+    n_colors: int = 0
+    color_count: np.ndarray | None = None  # [n_colors] elements per colour
+    color_start: np.ndarray | None = None  # [n_colors + 1] first position of each colour in color_elems
+    color_elems: np.ndarray | None = None  # [n_elem] element ids grouped by colour, ascending inside one
+
+
+def color_groups(color_of: np.ndarray):
+    """(n_colors, color_count, color_start, color_elems) of 1-based colours, in
+    the order of build_color_groups (RT_Asm_Color.f90:148-180): a colour's
+    elements in ascending id, all 1-based."""
+    color_of = np.asarray(color_of, dtype=np.int32)
+    n = int(color_of.max()) if color_of.size else 0
+    count = np.bincount(color_of - 1, minlength=n).astype(np.int32)
+    start = np.empty(n + 1, dtype=np.int32)
+    start[0] = 1
+    np.cumsum(count, out=start[1:])
+    start[1:] += 1
+    elems = (np.argsort(color_of, kind="stable") + 1).astype(np.int32)
+    return n, count, start, elems
+
+
+def RT_AsmColor_Build(ctx: NM_Solver_Ctx, result: RT_AsmColor_Result) -> ErrorStatusType:
+    """RT_AsmColor_Build (RT_Asm_Color.f90:36-146): the greedy colouring of the
+    model's elements (ascending order, smallest colour no element sharing a node
+    already has), as ufc_pattern_build computed it on the device, with the
+    colour groups."""
+    colours, status = _run("RT_AsmColor_Build", ctx.model.colors, 1)
+    if colours is not None:
+        result.color_of = colours
+        result.n_colors, result.color_count, result.color_start, result.color_elems = color_groups(colours)
+    return status
+
+
 def RT_Asm_GlobalStiffness(ctx: NM_Solver_Ctx, build=A.BUILD_FP64) -> ErrorStatusType:
     """RT_Asm_GlobalStiffness (ufc_core/L5_RT/Assembly/RT_Asm_Solv.f90:1762-1985):
     element loop and scatter into the CSR whose pattern the model built once."""
